@@ -1,0 +1,116 @@
+// Shared definitions of the cusmic_b200 kernels: border mapping, frame
+// descriptors, per-frame state, bit-plane layout and small device helpers.
+//
+// HBM layout of one call (all per frame, frames back to back):
+//   clean      float64 [h][w]      working pixels; the caller's output buffer
+//   bit planes uint32  [N_PLANES][h][words], words = ceil(w / 32); bit b of
+//              word (y, k) is pixel (y, 32 k + b); padding bits are zero
+//   targets    uint2   {frame, pixel} list of replacement targets
+#pragma once
+#include <cstdint>
+#include <cmath>
+#include <cuda_runtime.h>
+
+#if defined(__CUDACC__)
+#define CB_HD __host__ __device__ __forceinline__
+#else
+#define CB_HD inline
+#endif
+
+namespace cb {
+
+using std::fabs;
+using std::fmax;
+using std::fmin;
+using std::isfinite;
+using std::isnan;
+using std::sqrt;
+
+enum Border { REFLECT = 0, CONSTANT = 1, NEAREST = 2, MIRROR = 3, WRAP = 4 };
+
+// Bit planes of a frame.
+enum Plane {
+	P_HOLE,   // non-finite input pixel
+	P_EXCL,   // excluded from seeds and donors: hole or masked
+	P_DONOR,  // static donor: not excluded and finite after background
+	P_S1,     // significance > cr_threshold
+	P_S2,     // significance > neighbor_threshold
+	P_CAND,   // seed: S1, not excluded, contrast test passed
+	P_CRMASK, // cumulative cosmic-ray mask
+	N_PLANES
+};
+
+constexpr double FINE_FLOOR = 0.01;   // reference src/filters.cuh:21
+constexpr double SIGNAL_FLOOR = 1e-5; // reference src/filters.cuh:22
+
+// scipy.ndimage border conventions, reference src/filters.cuh:24-44: returns
+// the in-range index a coordinate reads, or -1 for a constant (zero) pad.
+CB_HD int border_index(int x, int n, int mode)
+{
+	if (x >= 0 && x < n)
+		return x;
+	if (mode == CONSTANT)
+		return -1;
+	if (mode == NEAREST)
+		return x < 0 ? 0 : n - 1;
+	if (n == 1)
+		return 0;
+	int period = mode == REFLECT ? 2 * n : mode == MIRROR ? 2 * (n - 1) : n;
+	x %= period;
+	if (x < 0)
+		x += period;
+	if (mode == REFLECT && x >= n)
+		return period - x - 1;
+	if (mode == MIRROR && x >= n)
+		return period - x;
+	return x;
+}
+
+CB_HD int clampi(int x, int lo, int hi)
+{
+	return x < lo ? lo : x > hi ? hi : x;
+}
+
+// One frame of a (possibly ragged) batch, as the kernels see it.
+struct FrameDesc {
+	const double *data, *error, *gain_map, *rn_map, *bg_map;
+	const uint8_t *mask;
+	double *clean;     // working pixels, restored in place into the output
+	uint8_t *mask_out; // uint8 output mask
+	uint32_t *bits;    // N_PLANES planes of `plane` words
+	double gain, rn, bg;
+	long long plane;   // words per plane = h * words
+	int w, h, words, has_bg;
+};
+
+// Device-side control state of a frame.
+struct FrameState {
+	unsigned int active;  // the next detection pass runs for this frame
+	unsigned int replace; // this pass flagged new pixels: re-replace targets
+	unsigned int error;   // a target had no finite donor
+	unsigned int passes;  // detection passes run
+	unsigned long long todo, donors;          // this pass: new pixels, donors left
+	unsigned long long holes, allowed, finite; // from preparation
+};
+
+// Loop control shared by the per-pass kernels.
+struct Control {
+	unsigned long long n_targets; // length of the target list
+	unsigned long long n_holes;   // length of the hole list (front of the same buffer)
+	int iter;                     // detection passes issued so far
+	int maxiter;
+	int any_active;
+	int pad;
+};
+
+CB_HD uint32_t *plane_ptr(const FrameDesc &f, int p)
+{
+	return f.bits + (long long)p * f.plane;
+}
+
+CB_HD bool test_bit(const uint32_t *plane, int words, int x, int y)
+{
+	return (plane[(long long)y * words + (x >> 5)] >> (x & 31)) & 1u;
+}
+
+} // namespace cb

@@ -1,0 +1,827 @@
+// Host side of cusmic_b200: batch layout, workspace pool, launch sequence and
+// the C ABI of include/cusmic.h and include/cusmic_b200.h.
+//
+// One call = init -> prepare -> hole fill -> maxiter x (detect -> grow/update
+// -> control -> replace) -> restore, all on the caller's stream, with no host
+// synchronisation inside the loop: per-frame activity lives on the device and
+// kernels skip frames that stopped (the reference instead copies counts to the
+// host after every pass, src/cleaner.cuh:69-76,128-142).  Plans capture the
+// same sequence into a CUDA graph whose loop is a device-driven while node.
+#include "../../include/cusmic.h"
+#include "../../include/cusmic_b200.h"
+#include "common.cuh"
+#include "detect.cuh"
+#include "kernels.cuh"
+
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifndef CUSMIC_B200_VERSION
+#define CUSMIC_B200_VERSION "0.1.0-b200"
+#endif
+
+namespace cb {
+
+struct InvalidArgument : std::invalid_argument {
+	using std::invalid_argument::invalid_argument;
+};
+
+static void check(cudaError_t e)
+{
+	if (e == cudaErrorMemoryAllocation)
+		throw std::bad_alloc();
+	if (e != cudaSuccess)
+		throw std::runtime_error(cudaGetErrorString(e));
+}
+
+constexpr int TILE_W = 32, TILE_H = 32, DETECT_THREADS = 256;
+using Tile = DetectTile<TILE_W, TILE_H>;
+#define DETECT_KERNEL detect_kernel<TILE_W, TILE_H, DETECT_THREADS>
+
+template <class T> struct DevBuf {
+	T *p = nullptr;
+	size_t n = 0;
+	DevBuf() = default;
+	DevBuf(const DevBuf &) = delete;
+	DevBuf &operator=(const DevBuf &) = delete;
+	void ensure(size_t want)
+	{
+		if (want <= n)
+			return;
+		if (p)
+			cudaFree(p);
+		p = nullptr;
+		n = 0;
+		if (want > SIZE_MAX / sizeof(T))
+			throw std::bad_alloc();
+		check(cudaMalloc(&p, want * sizeof(T)));
+		n = want;
+	}
+	~DevBuf()
+	{
+		if (p)
+			cudaFree(p);
+	}
+};
+
+template <class T> struct PinBuf {
+	T *p = nullptr;
+	size_t n = 0;
+	PinBuf() = default;
+	PinBuf(const PinBuf &) = delete;
+	PinBuf &operator=(const PinBuf &) = delete;
+	void ensure(size_t want)
+	{
+		if (want <= n)
+			return;
+		if (p)
+			cudaFreeHost(p);
+		p = nullptr;
+		n = 0;
+		check(cudaMallocHost(&p, want * sizeof(T)));
+		n = want;
+	}
+	~PinBuf()
+	{
+		if (p)
+			cudaFreeHost(p);
+	}
+};
+
+// Host description of one batch.
+struct Layout {
+	std::vector<FrameDesc> frames;
+	std::vector<long long> bit_off; // word offset of each frame's planes
+	std::vector<int4> tiles;
+	std::vector<int2> rows;
+	long long total_words = 0;
+	size_t total_px = 0;
+	DetectParams prm{};
+	int maxiter = 0;
+};
+
+struct DeviceInfo {
+	int sms = 0, detect_blocks_per_sm = 0;
+};
+
+static DeviceInfo device_info(int dev)
+{
+	static std::mutex mu;
+	static std::vector<DeviceInfo> cache;
+	std::lock_guard<std::mutex> lock(mu);
+	if ((int)cache.size() <= dev)
+		cache.resize(dev + 1);
+	DeviceInfo &d = cache[dev];
+	if (!d.sms) {
+		check(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+		check(cudaFuncSetAttribute(DETECT_KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)sizeof(Tile)));
+		check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.detect_blocks_per_sm,
+			DETECT_KERNEL, DETECT_THREADS, sizeof(Tile)));
+		if (d.detect_blocks_per_sm < 1)
+			d.detect_blocks_per_sm = 1;
+	}
+	return d;
+}
+
+struct Workspace {
+	int device = -1;
+	DevBuf<FrameDesc> frames;
+	DevBuf<FrameState> state;
+	DevBuf<int4> tiles;
+	DevBuf<int2> rows;
+	DevBuf<uint32_t> bits;
+	DevBuf<uint2> targets;
+	DevBuf<Control> ctl;
+	PinBuf<unsigned char> stage;
+	PinBuf<FrameState> hstate;
+	// Host-API staging of inputs and outputs.
+	DevBuf<double> hdata, herror, hgain, hrn, hbg, hclean;
+	DevBuf<uint8_t> hmask, hout;
+};
+
+static std::mutex pool_mu;
+static std::vector<std::unique_ptr<Workspace>> pool;
+
+struct Lease {
+	std::unique_ptr<Workspace> ws;
+	explicit Lease(int dev)
+	{
+		std::lock_guard<std::mutex> lock(pool_mu);
+		for (auto it = pool.begin(); it != pool.end(); ++it)
+			if ((*it)->device == dev) {
+				ws = std::move(*it);
+				pool.erase(it);
+				break;
+			}
+		if (!ws) {
+			ws.reset(new Workspace);
+			ws->device = dev;
+		}
+	}
+	~Lease()
+	{
+		if (!ws)
+			return;
+		std::lock_guard<std::mutex> lock(pool_mu);
+		pool.push_back(std::move(ws));
+	}
+	Workspace *operator->() { return ws.get(); }
+	Workspace &operator*() { return *ws; }
+};
+
+// Options and scalars of frame f after per-frame overrides.
+struct FrameScalars {
+	double gain, rn, bg;
+};
+
+static FrameScalars scalars_for(const cusmic_options &o, const cusmic_frame_scalars *sc, size_t f)
+{
+	FrameScalars r{o.gain, o.readnoise, o.background};
+	if (sc) {
+		if (!std::isnan(sc[f].gain))
+			r.gain = sc[f].gain;
+		if (!std::isnan(sc[f].readnoise))
+			r.rn = sc[f].readnoise;
+		r.bg = sc[f].background;
+	}
+	return r;
+}
+
+// Reference src/api.cu:47-81, generalised to ragged shapes and per-frame
+// scalars.  Messages match the reference's.
+static void check_arguments(const cusmic_image *ims, size_t nf, const cusmic_options *o,
+	const cusmic_frame_scalars *sc, const void *clean, const void *mask, bool same_shape)
+{
+	if (!ims || !o || !clean || !mask || !nf || nf > 65535)
+		throw InvalidArgument("invalid images, batch size or output buffers");
+	const size_t w0 = ims[0].width, h0 = ims[0].height;
+	size_t total = 0;
+	for (size_t f = 0; f < (same_shape ? 1 : nf); ++f) {
+		size_t w = ims[f].width, h = ims[f].height;
+		if (!w || !h || w > size_t(INT_MAX) / 4 / h)
+			throw InvalidArgument("invalid image dimensions");
+		size_t n = w * h;
+		if ((same_shape && nf > SIZE_MAX / sizeof(double) / n) ||
+			total > SIZE_MAX / sizeof(double) - n)
+			throw InvalidArgument("batch is too large");
+		total += n;
+	}
+	if (o->maxiter < 0 || o->border < 0 || o->border > CUSMIC_WRAP || !std::isfinite(o->contrast) ||
+		o->contrast < 0 || !std::isfinite(o->cr_threshold) || o->cr_threshold < 0 ||
+		!std::isfinite(o->neighbor_threshold) || o->neighbor_threshold < 0)
+		throw InvalidArgument("invalid detection settings");
+	for (size_t f = 0; f < nf; ++f) {
+		const cusmic_image &im = ims[f];
+		if (!im.data || (same_shape && (im.width != w0 || im.height != h0)))
+			throw InvalidArgument("frames must have data and the same shape");
+		FrameScalars s = scalars_for(*o, sc, f);
+		if (!im.error) {
+			bool needs_gain = o->maxiter || !std::isnan(s.gain);
+			if (!im.gain && needs_gain && (!std::isfinite(s.gain) || s.gain <= 0))
+				throw InvalidArgument("positive gain or error is required");
+			if (!im.readnoise && (!std::isfinite(s.rn) || s.rn < 0))
+				throw InvalidArgument("read noise must be finite and nonnegative");
+		}
+		if (!im.background && !std::isnan(s.bg) && !std::isfinite(s.bg))
+			throw InvalidArgument("background must be finite");
+	}
+}
+
+static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
+	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask)
+{
+	Layout L;
+	L.maxiter = o.maxiter;
+	L.prm.contrast = o.contrast;
+	L.prm.cr = o.cr_threshold;
+	L.prm.nb = o.neighbor_threshold;
+	L.prm.tmin = std::fmin(o.cr_threshold, o.neighbor_threshold);
+	L.prm.mode = o.border;
+	L.frames.resize(nf);
+	L.bit_off.resize(nf);
+	size_t px = 0;
+	long long words = 0;
+	for (size_t f = 0; f < nf; ++f) {
+		const cusmic_image &im = ims[f];
+		FrameDesc &d = L.frames[f];
+		FrameScalars s = scalars_for(o, sc, f);
+		d.data = im.data;
+		d.error = im.error;
+		d.gain_map = im.error ? nullptr : im.gain;
+		d.rn_map = im.error ? nullptr : im.readnoise;
+		d.bg_map = im.background;
+		d.mask = im.mask;
+		d.clean = clean + px;
+		d.mask_out = mask + px;
+		d.gain = s.gain;
+		d.rn = s.rn;
+		d.bg = s.bg;
+		d.w = (int)im.width;
+		d.h = (int)im.height;
+		d.words = (d.w + 31) / 32;
+		d.plane = (long long)d.h * d.words;
+		d.has_bg = im.background != nullptr || !std::isnan(s.bg);
+		d.bits = nullptr;
+		L.bit_off[f] = words;
+		words += (long long)N_PLANES * d.plane;
+		px += (size_t)d.w * d.h;
+		for (int y = 0; y < d.h; ++y)
+			L.rows.push_back(make_int2((int)f, y));
+		for (int ty = 0; ty < d.h; ty += TILE_H)
+			for (int tx = 0; tx < d.w; tx += TILE_W)
+				L.tiles.push_back(make_int4((int)f, tx, ty, 0));
+	}
+	L.total_px = px;
+	L.total_words = words;
+	return L;
+}
+
+static int grid_for_rows(const DeviceInfo &di, size_t nrows)
+{
+	size_t blocks = (nrows + 7) / 8;
+	size_t cap = (size_t)di.sms * 8;
+	return (int)(blocks < 1 ? 1 : blocks > cap ? cap : blocks);
+}
+
+// Allocate the workspace for L and upload descriptors (stream-ordered).
+static void upload(Workspace &ws, Layout &L, cudaStream_t s)
+{
+	const size_t nf = L.frames.size();
+	ws.frames.ensure(nf);
+	ws.state.ensure(nf);
+	ws.tiles.ensure(L.tiles.size() ? L.tiles.size() : 1);
+	ws.rows.ensure(L.rows.size());
+	ws.ctl.ensure(1);
+	if (L.maxiter) {
+		ws.bits.ensure((size_t)L.total_words);
+		ws.targets.ensure(L.total_px);
+	}
+	for (size_t f = 0; f < nf; ++f)
+		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
+	size_t bytes_f = nf * sizeof(FrameDesc), bytes_t = L.tiles.size() * sizeof(int4);
+	size_t bytes_r = L.rows.size() * sizeof(int2);
+	ws.stage.ensure(bytes_f + bytes_t + bytes_r);
+	// The previous call using this workspace synchronised before returning,
+	// so the staging buffer is free.
+	std::memcpy(ws.stage.p, L.frames.data(), bytes_f);
+	std::memcpy(ws.stage.p + bytes_f, L.tiles.data(), bytes_t);
+	std::memcpy(ws.stage.p + bytes_f + bytes_t, L.rows.data(), bytes_r);
+	check(cudaMemcpyAsync(ws.frames.p, ws.stage.p, bytes_f, cudaMemcpyHostToDevice, s));
+	if (bytes_t)
+		check(cudaMemcpyAsync(ws.tiles.p, ws.stage.p + bytes_f, bytes_t, cudaMemcpyHostToDevice, s));
+	check(cudaMemcpyAsync(ws.rows.p, ws.stage.p + bytes_f + bytes_t, bytes_r,
+		cudaMemcpyHostToDevice, s));
+}
+
+struct GraphLoop {
+	cudaGraphConditionalHandle handle = 0;
+	bool use = false;
+};
+
+// Kernel kinds reported by cusmic_plan_profile().
+enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_DETECT, K_GROW, K_CONTROL, K_REPLACE, K_RESTORE,
+	K_COPY, K_KINDS };
+
+// Optional CUDA-event timer: an event after every launch on the launching
+// stream, so each kernel's duration is the gap to the previous event.
+struct Recorder {
+	std::vector<cudaEvent_t> events;
+	std::vector<int> kinds;
+	cudaStream_t s = nullptr;
+	void begin(cudaStream_t stream)
+	{
+		s = stream;
+		mark(-1);
+	}
+	void mark(int kind)
+	{
+		cudaEvent_t e;
+		check(cudaEventCreate(&e));
+		check(cudaEventRecord(e, s));
+		events.push_back(e);
+		kinds.push_back(kind);
+	}
+	~Recorder()
+	{
+		for (cudaEvent_t e : events)
+			cudaEventDestroy(e);
+	}
+};
+
+static inline void mark(Recorder *r, int kind)
+{
+	if (r)
+		r->mark(kind);
+}
+
+static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
+	const GraphLoop &gl, Recorder *rec = nullptr)
+{
+	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size(), ntiles = (int)L.tiles.size();
+	int dblocks = di.sms * di.detect_blocks_per_sm;
+	if (dblocks > ntiles)
+		dblocks = ntiles;
+	DETECT_KERNEL<<<dblocks, DETECT_THREADS, sizeof(Tile), s>>>(ws.frames.p, ws.state.p,
+		ws.tiles.p, ntiles, L.prm);
+	mark(rec, K_DETECT);
+	grow_update_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p,
+		ws.rows.p, nrows, ws.targets.p, ws.ctl.p);
+	mark(rec, K_GROW);
+	control_kernel<<<1, 1024, 0, s>>>(ws.state.p, nf, ws.ctl.p, gl.handle, gl.use ? 1 : 0);
+	mark(rec, K_CONTROL);
+	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
+		&ws.ctl.p->n_targets, 0);
+	mark(rec, K_REPLACE);
+}
+
+static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
+	Recorder *rec = nullptr)
+{
+	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
+	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter);
+	mark(rec, K_INIT);
+	if (!L.maxiter) {
+		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
+		mark(rec, K_COPY);
+		return;
+	}
+	prepare_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
+		nrows, ws.targets.p, ws.ctl.p);
+	mark(rec, K_PREPARE);
+	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
+		&ws.ctl.p->n_holes, 1);
+	mark(rec, K_FILL);
+}
+
+static void launch_epilogue(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
+	Recorder *rec = nullptr)
+{
+	if (!L.maxiter)
+		return;
+	const int nrows = (int)L.rows.size();
+	restore_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
+	mark(rec, K_RESTORE);
+}
+
+// Whole cleaning on stream s without graphs.
+static void enqueue_plain(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
+	Recorder *rec = nullptr)
+{
+	if (rec)
+		rec->begin(s);
+	launch_prologue(ws, L, di, s, rec);
+	for (int it = 0; it < L.maxiter; ++it)
+		launch_pass(ws, L, di, s, GraphLoop{}, rec);
+	launch_epilogue(ws, L, di, s, rec);
+	check(cudaGetLastError());
+}
+
+// Copy per-frame state back and turn it into a status (stream must be idle
+// after this returns).
+static void finish(Workspace &ws, size_t nf, cudaStream_t s, std::vector<int> *passes = nullptr)
+{
+	ws.hstate.ensure(nf);
+	check(cudaMemcpyAsync(ws.hstate.p, ws.state.p, nf * sizeof(FrameState), cudaMemcpyDeviceToHost, s));
+	check(cudaStreamSynchronize(s));
+	check(cudaGetLastError());
+	if (passes)
+		passes->assign(nf, 0);
+	for (size_t f = 0; f < nf; ++f) {
+		const FrameState &st = ws.hstate.p[f];
+		if (passes)
+			(*passes)[f] = (int)st.passes;
+		if (st.error || (st.holes && st.allowed && !st.finite))
+			throw InvalidArgument("no finite replacement donors");
+	}
+}
+
+template <class F> static int guarded(F run, char *msg, size_t len)
+{
+	if (msg && len)
+		msg[0] = 0;
+	try {
+		run();
+		return CUSMIC_OK;
+	} catch (const std::invalid_argument &e) {
+		if (msg && len)
+			std::snprintf(msg, len, "%s", e.what());
+		return CUSMIC_INVALID;
+	} catch (const std::bad_alloc &e) {
+		if (msg && len)
+			std::snprintf(msg, len, "%s", e.what());
+		return CUSMIC_NO_MEMORY;
+	} catch (const std::exception &e) {
+		if (msg && len)
+			std::snprintf(msg, len, "%s", e.what());
+		return CUSMIC_CUDA_ERROR;
+	} catch (...) {
+		if (msg && len)
+			std::snprintf(msg, len, "unknown error");
+		return CUSMIC_CUDA_ERROR;
+	}
+}
+
+static void run_device(const cusmic_image *ims, size_t nf, const cusmic_options &o,
+	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask, cudaStream_t s,
+	std::vector<int> *passes = nullptr)
+{
+	int dev;
+	check(cudaGetDevice(&dev));
+	DeviceInfo di = device_info(dev);
+	Layout L = make_layout(ims, nf, o, sc, clean, mask);
+	Lease ws(dev);
+	upload(*ws, L, s);
+	enqueue_plain(*ws, L, di, s);
+	finish(*ws, nf, s, passes);
+}
+
+// Reference src/api.cu:107-114.
+static void check_values(const double *data, size_t n, const char *name, int minimum)
+{
+	for (size_t i = 0; data && i < n; ++i)
+		if (!std::isfinite(data[i]) || (minimum == 1 && data[i] <= 0) ||
+			(minimum == 0 && data[i] < 0))
+			throw InvalidArgument(name);
+}
+
+} // namespace cb
+
+using namespace cb;
+
+extern "C" const char *cusmic_version(void)
+{
+	return CUSMIC_B200_VERSION;
+}
+
+extern "C" int cusmic_cuda_version(void)
+{
+	return CUDART_VERSION;
+}
+
+extern "C" void cusmic_default_options(cusmic_options *options)
+{
+	if (options)
+		*options = {3, 5, 3, NAN, 0, NAN, 4, CUSMIC_MIRROR};
+}
+
+extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, double *clean,
+	uint8_t *mask, char *msg, size_t len)
+{
+	return guarded([&] {
+		check_arguments(im, 1, o, nullptr, clean, mask, true);
+		const size_t n = im->width * im->height;
+		if (im->error)
+			check_values(im->error, n, "error must be finite and positive", 1);
+		else {
+			check_values(im->gain, n, "gain must be finite and positive", 1);
+			check_values(im->readnoise, n, "read noise must be finite and nonnegative", 0);
+		}
+		check_values(im->background, n, "background must be finite", -1);
+
+		int dev;
+		check(cudaGetDevice(&dev));
+		Lease ws(dev);
+		const double *gmap = im->error ? nullptr : im->gain;
+		const double *rnmap = im->error ? nullptr : im->readnoise;
+		ws->hdata.ensure(n);
+		ws->hclean.ensure(n);
+		ws->hout.ensure(n);
+		cudaStream_t s = nullptr;
+		check(cudaMemcpyAsync(ws->hdata.p, im->data, n * sizeof(double), cudaMemcpyHostToDevice, s));
+		cusmic_image gpu = *im;
+		gpu.data = ws->hdata.p;
+		auto stage = [&](DevBuf<double> &b, const double *src) -> const double * {
+			if (!src)
+				return nullptr;
+			b.ensure(n);
+			check(cudaMemcpyAsync(b.p, src, n * sizeof(double), cudaMemcpyHostToDevice, s));
+			return b.p;
+		};
+		gpu.error = stage(ws->herror, im->error);
+		gpu.gain = stage(ws->hgain, gmap);
+		gpu.readnoise = stage(ws->hrn, rnmap);
+		gpu.background = stage(ws->hbg, im->background);
+		if (im->mask) {
+			ws->hmask.ensure(n);
+			check(cudaMemcpyAsync(ws->hmask.p, im->mask, n, cudaMemcpyHostToDevice, s));
+			gpu.mask = ws->hmask.p;
+		}
+		DeviceInfo di = device_info(dev);
+		Layout L = make_layout(&gpu, 1, *o, nullptr, ws->hclean.p, ws->hout.p);
+		upload(*ws, L, s);
+		enqueue_plain(*ws, L, di, s);
+		finish(*ws, 1, s);
+		check(cudaMemcpy(clean, ws->hclean.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+		check(cudaMemcpy(mask, ws->hout.p, n, cudaMemcpyDeviceToHost));
+	}, msg, len);
+}
+
+extern "C" int remove_cosmics_batch_device(const cusmic_image *ims, size_t nf,
+	const cusmic_options *o, double *clean, uint8_t *mask, void *stream, char *msg, size_t len)
+{
+	return guarded([&] {
+		check_arguments(ims, nf, o, nullptr, clean, mask, true);
+		run_device(ims, nf, *o, nullptr, clean, mask, (cudaStream_t)stream);
+	}, msg, len);
+}
+
+extern "C" int remove_cosmics_device(const cusmic_image *im, const cusmic_options *o, double *clean,
+	uint8_t *mask, void *stream, char *msg, size_t len)
+{
+	return remove_cosmics_batch_device(im, 1, o, clean, mask, stream, msg, len);
+}
+
+extern "C" int cusmic_ragged_batch_device(const cusmic_image *ims, size_t nf,
+	const cusmic_options *o, const cusmic_frame_scalars *sc, double *clean, uint8_t *mask,
+	void *stream, char *msg, size_t len)
+{
+	return guarded([&] {
+		check_arguments(ims, nf, o, sc, clean, mask, false);
+		run_device(ims, nf, *o, sc, clean, mask, (cudaStream_t)stream);
+	}, msg, len);
+}
+
+// ---------------------------------------------------------------------------
+// Plans: a fixed batch with its own workspace, descriptors uploaded once, and
+// optionally the whole cleaning captured as one CUDA graph.  The maxiter loop
+// becomes a conditional WHILE node whose condition control_kernel sets from
+// the device (any frame still active and passes left), so the early exit costs
+// no host round trip.
+
+struct cusmic_plan {
+	int device = -1;
+	int flags = 0;
+	Layout L;
+	DeviceInfo di;
+	Workspace ws;
+	cusmic_options options{};
+	std::vector<cusmic_image> ims;
+	std::vector<cusmic_frame_scalars> scalars;
+	cudaStream_t private_stream = nullptr;
+	cudaStream_t last = nullptr;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	bool executed = false;
+
+	~cusmic_plan()
+	{
+		if (exec)
+			cudaGraphExecDestroy(exec);
+		if (graph)
+			cudaGraphDestroy(graph);
+		if (private_stream)
+			cudaStreamDestroy(private_stream);
+	}
+};
+
+namespace cb {
+
+static void capture_graph(cusmic_plan &p)
+{
+	cudaStream_t cs = p.private_stream;
+	check(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+	try {
+		launch_prologue(p.ws, p.L, p.di, cs);
+		if (p.L.maxiter) {
+			cudaStreamCaptureStatus st;
+			cudaGraph_t g;
+			const cudaGraphNode_t *deps = nullptr;
+			size_t nd = 0;
+			check(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
+			cudaGraphConditionalHandle handle;
+			check(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+			cudaGraphNodeParams cp = {};
+			cp.type = cudaGraphNodeTypeConditional;
+			cp.conditional.handle = handle;
+			cp.conditional.type = cudaGraphCondTypeWhile;
+			cp.conditional.size = 1;
+			cudaGraphNode_t node;
+			check(cudaGraphAddNode(&node, g, deps, nd, &cp));
+			cudaGraph_t body = cp.conditional.phGraph_out[0];
+			check(cudaStreamUpdateCaptureDependencies(cs, &node, 1,
+				cudaStreamSetCaptureDependencies));
+			cudaStream_t bs;
+			check(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+			cudaError_t err = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
+				cudaStreamCaptureModeThreadLocal);
+			if (err == cudaSuccess) {
+				launch_pass(p.ws, p.L, p.di, bs, GraphLoop{handle, true});
+				err = cudaStreamEndCapture(bs, nullptr);
+			}
+			cudaStreamDestroy(bs);
+			check(err);
+		}
+		launch_epilogue(p.ws, p.L, p.di, cs);
+	} catch (...) {
+		cudaGraph_t g = nullptr;
+		cudaStreamEndCapture(cs, &g);
+		if (g)
+			cudaGraphDestroy(g);
+		throw;
+	}
+	check(cudaStreamEndCapture(cs, &p.graph));
+	check(cudaGraphInstantiate(&p.exec, p.graph, 0));
+}
+
+static void plan_upload(cusmic_plan &p)
+{
+	upload(p.ws, p.L, p.private_stream);
+	check(cudaStreamSynchronize(p.private_stream));
+}
+
+} // namespace cb
+
+extern "C" int cusmic_plan_create(cusmic_plan **out, const cusmic_image *ims, size_t nf,
+	const cusmic_options *o, const cusmic_frame_scalars *sc, double *clean, uint8_t *mask,
+	int flags, char *msg, size_t len)
+{
+	return guarded([&] {
+		if (!out)
+			throw InvalidArgument("invalid plan pointer");
+		*out = nullptr;
+		check_arguments(ims, nf, o, sc, clean, mask, false);
+		std::unique_ptr<cusmic_plan> p(new cusmic_plan);
+		check(cudaGetDevice(&p->device));
+		p->flags = flags;
+		p->di = device_info(p->device);
+		p->options = *o;
+		p->ims.assign(ims, ims + nf);
+		if (sc)
+			p->scalars.assign(sc, sc + nf);
+		p->L = make_layout(ims, nf, *o, sc, clean, mask);
+		check(cudaStreamCreateWithFlags(&p->private_stream, cudaStreamNonBlocking));
+		plan_upload(*p);
+		if (flags & CUSMIC_PLAN_GRAPH)
+			capture_graph(*p);
+		*out = p.release();
+	}, msg, len);
+}
+
+extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double *clean,
+	uint8_t *mask, char *msg, size_t len)
+{
+	return guarded([&] {
+		if (!p || !ims || !clean || !mask)
+			throw InvalidArgument("invalid plan or buffers");
+		const size_t nf = p->ims.size();
+		for (size_t f = 0; f < nf; ++f) {
+			const cusmic_image &a = ims[f], &b = p->ims[f];
+			if (!a.data || a.width != b.width || a.height != b.height ||
+				!a.error != !b.error || !a.gain != !b.gain || !a.readnoise != !b.readnoise ||
+				!a.background != !b.background || !a.mask != !b.mask)
+				throw InvalidArgument("frames must keep the plan's shapes and maps");
+		}
+		if (p->last)
+			check(cudaStreamSynchronize(p->last));
+		Layout L = make_layout(ims, nf, p->options, p->scalars.empty() ? nullptr : p->scalars.data(),
+			clean, mask);
+		for (size_t f = 0; f < nf; ++f)
+			L.frames[f].bits = p->L.frames[f].bits;
+		p->ims.assign(ims, ims + nf);
+		p->L.frames = L.frames;
+		const size_t bytes = nf * sizeof(FrameDesc);
+		std::memcpy(p->ws.stage.p, p->L.frames.data(), bytes);
+		check(cudaMemcpyAsync(p->ws.frames.p, p->ws.stage.p, bytes, cudaMemcpyHostToDevice,
+			p->private_stream));
+		check(cudaStreamSynchronize(p->private_stream));
+	}, msg, len);
+}
+
+extern "C" int cusmic_plan_execute(cusmic_plan *p, void *stream, char *msg, size_t len)
+{
+	return guarded([&] {
+		if (!p)
+			throw InvalidArgument("invalid plan");
+		cudaStream_t s = (cudaStream_t)stream;
+		if (p->exec)
+			check(cudaGraphLaunch(p->exec, s));
+		else
+			enqueue_plain(p->ws, p->L, p->di, s);
+		const size_t nf = p->L.frames.size();
+		p->ws.hstate.ensure(nf);
+		check(cudaMemcpyAsync(p->ws.hstate.p, p->ws.state.p, nf * sizeof(FrameState),
+			cudaMemcpyDeviceToHost, s));
+		p->last = s;
+		p->executed = true;
+	}, msg, len);
+}
+
+extern "C" int cusmic_plan_wait(cusmic_plan *p, char *msg, size_t len)
+{
+	return guarded([&] {
+		if (!p || !p->executed)
+			throw InvalidArgument("plan has not been executed");
+		check(cudaStreamSynchronize(p->last));
+		check(cudaGetLastError());
+		for (size_t f = 0; f < p->L.frames.size(); ++f) {
+			const FrameState &st = p->ws.hstate.p[f];
+			if (st.error || (st.holes && st.allowed && !st.finite))
+				throw InvalidArgument("no finite replacement donors");
+		}
+	}, msg, len);
+}
+
+extern "C" int cusmic_plan_passes(cusmic_plan *p, int *passes)
+{
+	if (!p || !passes || !p->executed)
+		return CUSMIC_INVALID;
+	if (cudaStreamSynchronize(p->last) != cudaSuccess)
+		return CUSMIC_CUDA_ERROR;
+	for (size_t f = 0; f < p->L.frames.size(); ++f)
+		passes[f] = (int)p->ws.hstate.p[f].passes;
+	return CUSMIC_OK;
+}
+
+extern "C" void cusmic_plan_destroy(cusmic_plan *p)
+{
+	if (!p)
+		return;
+	if (p->last)
+		cudaStreamSynchronize(p->last);
+	delete p;
+}
+
+extern "C" int cusmic_plan_profile(cusmic_plan *p, void *stream, double *ms, int *launches,
+	int kinds, char *msg, size_t len)
+{
+	return guarded([&] {
+		if (!p || !ms || !launches || kinds < K_KINDS)
+			throw InvalidArgument("invalid plan or profile buffers");
+		cudaStream_t s = (cudaStream_t)stream;
+		Recorder rec;
+		enqueue_plain(p->ws, p->L, p->di, s, &rec);
+		const size_t nf = p->L.frames.size();
+		p->ws.hstate.ensure(nf);
+		check(cudaMemcpyAsync(p->ws.hstate.p, p->ws.state.p, nf * sizeof(FrameState),
+			cudaMemcpyDeviceToHost, s));
+		p->last = s;
+		p->executed = true;
+		check(cudaStreamSynchronize(s));
+		for (int k = 0; k < kinds; ++k) {
+			ms[k] = 0;
+			launches[k] = 0;
+		}
+		for (size_t i = 1; i < rec.events.size(); ++i) {
+			float t = 0;
+			check(cudaEventElapsedTime(&t, rec.events[i - 1], rec.events[i]));
+			ms[rec.kinds[i]] += t;
+			launches[rec.kinds[i]] += 1;
+		}
+	}, msg, len);
+}
+
+extern "C" int cusmic_plan_backward(cusmic_plan *p, const double *grad_clean, double *grad_data,
+	double *grad_background, void *stream, char *msg, size_t len)
+{
+	(void)p, (void)grad_clean, (void)grad_data, (void)grad_background, (void)stream;
+	return guarded([&] { throw InvalidArgument("backward is not available in this build"); }, msg, len);
+}

@@ -1,0 +1,462 @@
+// Per-pass kernels around the detection kernel: preparation, bit-packed growth
+// and mask update, loop control, replacement, restoration.
+//
+// Row kernels give one warp a frame row at a time (a row-item list of
+// {frame, y} covers ragged batches), so each warp instruction reads 32
+// consecutive float64 pixels and the bit planes fall out of __ballot_sync.
+#pragma once
+#include "common.cuh"
+#include "select.cuh"
+
+namespace cb {
+
+__device__ __forceinline__ int warp_sum_int(int v)
+{
+#pragma unroll
+	for (int o = 16; o; o >>= 1)
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
+{
+#pragma unroll
+	for (int o = 16; o; o >>= 1)
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// Append `cnt` entries per lane to a global list; returns this lane's first slot.
+__device__ __forceinline__ unsigned long long warp_append(unsigned long long *counter, int cnt)
+{
+	const int lane = threadIdx.x & 31;
+	int incl = cnt;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		int v = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o)
+			incl += v;
+	}
+	int total = __shfl_sync(0xffffffffu, incl, 31);
+	unsigned long long base = 0;
+	if (lane == 31 && total)
+		base = atomicAdd(counter, (unsigned long long)total);
+	base = __shfl_sync(0xffffffffu, base, 31);
+	return base + (unsigned long long)(incl - cnt);
+}
+
+__global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < nf) {
+		FrameState s = {};
+		s.active = maxiter > 0;
+		state[i] = s;
+	}
+	if (i == 0) {
+		Control c = {};
+		c.maxiter = maxiter;
+		c.any_active = maxiter > 0;
+		*ctl = c;
+	}
+}
+
+// Reference src/image.cuh:24-48: holes, exclusions, clean = data (+ bg), the
+// static donor plane (the reference's is_donor with an empty mask), counts,
+// and the hole list for the initial fill (src/cleaner.cuh:78-100).
+__global__ void __launch_bounds__(256)
+prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
+	int nrows, uint2 *holes_out, Control *ctl)
+{
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int r = gw; r < nrows; r += nw) {
+		const int2 item = rows[r];
+		const FrameDesc &fd = frames[item.x];
+		const int w = fd.w, y = item.y, words = fd.words;
+		const long long rowpix = (long long)y * w, roww = (long long)y * words;
+		int holes = 0, allowed = 0, finite = 0;
+		for (int x0 = 0; x0 < w; x0 += 32) {
+			const int x = x0 + lane;
+			const bool valid = x < w;
+			const long long i = rowpix + x;
+			bool hole = false, ok = false, donor = false;
+			if (valid) {
+				double d = fd.data[i];
+				hole = !isfinite(d);
+				ok = !hole && !(fd.mask && fd.mask[i]);
+				double c = hole ? 0 : d;
+				if (fd.has_bg)
+					c += 1 * (fd.bg_map ? fd.bg_map[i] : fd.bg);
+				fd.clean[i] = c;
+				donor = ok && isfinite(c);
+			}
+			const uint32_t hw = __ballot_sync(0xffffffffu, hole);
+			const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
+			const uint32_t dw = __ballot_sync(0xffffffffu, donor);
+			const uint32_t aw = __ballot_sync(0xffffffffu, ok);
+			if (lane < N_PLANES) {
+				uint32_t v = lane == P_HOLE ? hw : lane == P_EXCL ? ew : lane == P_DONOR ? dw : 0u;
+				plane_ptr(fd, lane)[roww + (x0 >> 5)] = v;
+			}
+			holes += __popc(hw);
+			allowed += __popc(aw);
+			finite += __popc(dw);
+			if (hw) {
+				unsigned long long base = warp_append(&ctl->n_holes, hole ? 1 : 0);
+				if (hole)
+					holes_out[base] = make_uint2((unsigned)item.x, (unsigned)i);
+			}
+		}
+		if (lane == 0) {
+			if (holes)
+				atomicAdd(&state[item.x].holes, (unsigned long long)holes);
+			if (allowed)
+				atomicAdd(&state[item.x].allowed, (unsigned long long)allowed);
+			if (finite)
+				atomicAdd(&state[item.x].finite, (unsigned long long)finite);
+		}
+	}
+}
+
+// 36-bit window of a bit-plane row around word k: bits 0..35 are pixels
+// 32k-2 .. 32k+33 (zero outside the frame).
+__device__ __forceinline__ unsigned long long bit_window(const uint32_t *plane, int words, int h,
+	int y, int k)
+{
+	if (y < 0 || y >= h)
+		return 0;
+	const uint32_t *row = plane + (long long)y * words;
+	unsigned long long c = row[k];
+	unsigned long long l = k > 0 ? row[k - 1] : 0u;
+	unsigned long long r = k + 1 < words ? row[k + 1] : 0u;
+	return (l >> 30) | (c << 2) | ((r & 3ull) << 34);
+}
+
+__device__ __forceinline__ unsigned long long dilate_row(unsigned long long e)
+{
+	return e | (e << 1) | (e >> 1);
+}
+
+// Reference src/filters.cuh:177-193 twice (src/cleaner.cuh:123-125) and
+// src/cleaner.cuh:22-37: grown = dilate3x3(dilate3x3(cand) & S1) & S2 on bit
+// planes, fresh = grown & ~crmask, crmask |= grown, per-frame counts of fresh
+// pixels and remaining donors, and fresh pixels appended to the target list.
+__global__ void __launch_bounds__(256)
+grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
+	const int2 *__restrict__ rows, int nrows, uint2 *targets, Control *ctl)
+{
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int r = gw; r < nrows; r += nw) {
+		const int2 item = rows[r];
+		if (!state[item.x].active)
+			continue; // warp-uniform
+		const FrameDesc &fd = frames[item.x];
+		const int w = fd.w, h = fd.h, y = item.y, words = fd.words;
+		const uint32_t *cand = plane_ptr(fd, P_CAND), *s1 = plane_ptr(fd, P_S1);
+		const uint32_t *s2 = plane_ptr(fd, P_S2), *donor = plane_ptr(fd, P_DONOR);
+		uint32_t *crm = plane_ptr(fd, P_CRMASK);
+		unsigned long long todo = 0, donors = 0;
+		for (int k0 = 0; k0 < words; k0 += 32) {
+			const int k = k0 + lane;
+			uint32_t fresh = 0;
+			if (k < words) {
+				unsigned long long c[5], g1[3];
+#pragma unroll
+				for (int d = 0; d < 5; ++d)
+					c[d] = dilate_row(bit_window(cand, words, h, y - 2 + d, k));
+#pragma unroll
+				for (int d = 0; d < 3; ++d)
+					g1[d] = bit_window(s1, words, h, y - 1 + d, k) & (c[d] | c[d + 1] | c[d + 2]);
+				unsigned long long g2 = ((unsigned long long)s2[(long long)y * words + k] << 2) &
+					(dilate_row(g1[0]) | dilate_row(g1[1]) | dilate_row(g1[2]));
+				const uint32_t grown = (uint32_t)(g2 >> 2);
+				const long long o = (long long)y * words + k;
+				const uint32_t old = crm[o];
+				fresh = grown & ~old;
+				const uint32_t now = old | grown;
+				if (fresh)
+					crm[o] = now;
+				todo += __popc(fresh);
+				donors += __popc(donor[o] & ~now);
+			}
+			if (__any_sync(0xffffffffu, fresh != 0)) {
+				unsigned long long slot = warp_append(&ctl->n_targets, __popc(fresh));
+				const unsigned base = (unsigned)((long long)y * w + 32 * k);
+				while (fresh) {
+					int b = __ffs(fresh) - 1;
+					fresh &= fresh - 1;
+					targets[slot++] = make_uint2((unsigned)item.x, base + b);
+				}
+			}
+		}
+		todo = warp_sum_u64(todo);
+		donors = warp_sum_u64(donors);
+		if (lane == 0) {
+			if (todo)
+				atomicAdd(&state[item.x].todo, todo);
+			if (donors)
+				atomicAdd(&state[item.x].donors, donors);
+		}
+	}
+}
+
+// Per-frame loop control after a pass (reference src/cleaner.cuh:128-142,
+// 175-181): a frame with new pixels but no donors fails, a frame without new
+// pixels stops (its later passes would repeat this one), the others replace
+// and continue.  With a graph handle, sets the while-node condition.
+__global__ void __launch_bounds__(1024)
+control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHandle handle,
+	int use_handle)
+{
+	int any = 0;
+	for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+		FrameState s = state[f];
+		s.replace = 0;
+		if (s.active) {
+			++s.passes;
+			if (s.todo && !s.donors) {
+				s.error = 1;
+				s.active = 0;
+			} else if (s.todo) {
+				s.replace = 1;
+				any = 1;
+			} else {
+				s.active = 0;
+			}
+		}
+		s.todo = 0;
+		s.donors = 0;
+		state[f] = s;
+	}
+	any = __syncthreads_or(any);
+	if (threadIdx.x == 0) {
+		int it = ++ctl->iter;
+		ctl->any_active = any;
+		if (use_handle)
+			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
+	}
+}
+
+// IEEE bits mapped to an unsigned total order (reference src/replace.cuh:37-48).
+__device__ __forceinline__ unsigned long long order_key(double v)
+{
+	unsigned long long b = (unsigned long long)__double_as_longlong(v);
+	return (b >> 63) ? ~b : b ^ (1ull << 63);
+}
+
+__device__ __forceinline__ double order_value(unsigned long long k)
+{
+	return __longlong_as_double((long long)((k >> 63) ? k ^ (1ull << 63) : ~k));
+}
+
+// Reference src/replace.cuh:50-56.
+__device__ __forceinline__ double midpoint(double lo, double hi)
+{
+	if (fabs(lo) < 1 && fabs(hi) < 1)
+		return (lo + hi) / 2;
+	return lo / 2 + hi / 2;
+}
+
+// Ascending bitonic network over the 32 lanes with the reference's exchange
+// (src/replace.cuh:68-83): strict < comparisons, so equal values (such as -0
+// and +0) end in the same lanes as in the reference.
+__device__ __forceinline__ double bitonic32(double v)
+{
+	const int lane = threadIdx.x & 31;
+#pragma unroll
+	for (int span = 2; span <= 32; span *= 2) {
+#pragma unroll
+		for (int step = span / 2; step; step /= 2) {
+			double peer = __shfl_xor_sync(0xffffffffu, v, step);
+			bool lower = ((lane & span) == 0) == ((lane & step) == 0);
+			v = lower ? (peer < v ? peer : v) : (v < peer ? peer : v);
+		}
+	}
+	return v;
+}
+
+struct Window {
+	int x0, x1, y0, y1;
+};
+
+__device__ __forceinline__ bool donor_at(const uint32_t *don, const uint32_t *crm, int words,
+	int x, int y)
+{
+	long long o = (long long)y * words + (x >> 5);
+	return ((don[o] & ~crm[o]) >> (x & 31)) & 1u;
+}
+
+// The donor of rank `rank` in key order inside a window larger than 32 cells:
+// an MSB-first radix select over ordered 64-bit keys (same ranks as reference
+// src/replace.cuh:85-109).  Up to 8 cells per lane are kept in registers.
+__device__ double select_rank(const FrameDesc &fd, const uint32_t *don, const uint32_t *crm, Window win,
+	int rank)
+{
+	const int lane = threadIdx.x & 31;
+	const int ww = win.x1 - win.x0 + 1, area = ww * (win.y1 - win.y0 + 1);
+	unsigned long long prefix = 0, used = 0;
+	if (area <= 256) {
+		unsigned long long keys[8];
+		unsigned valid = 0;
+#pragma unroll
+		for (int s = 0; s < 8; ++s) {
+			int pos = lane + 32 * s;
+			keys[s] = 0;
+			if (pos < area) {
+				int x = win.x0 + pos % ww, y = win.y0 + pos / ww;
+				if (donor_at(don, crm, fd.words, x, y)) {
+					keys[s] = order_key(fd.clean[(long long)y * fd.w + x]);
+					valid |= 1u << s;
+				}
+			}
+		}
+		for (int bit = 63; bit >= 0; --bit) {
+			const unsigned long long flag = 1ull << bit;
+			int below = 0;
+#pragma unroll
+			for (int s = 0; s < 8; ++s)
+				below += ((valid >> s) & 1u) && (keys[s] & used) == prefix && !(keys[s] & flag);
+			below = warp_sum_int(below);
+			used |= flag;
+			if (rank >= below) {
+				prefix |= flag;
+				rank -= below;
+			}
+		}
+		return order_value(prefix);
+	}
+	for (int bit = 63; bit >= 0; --bit) {
+		const unsigned long long flag = 1ull << bit;
+		int below = 0;
+		for (int pos = lane; pos < area; pos += 32) {
+			int x = win.x0 + pos % ww, y = win.y0 + pos / ww;
+			if (!donor_at(don, crm, fd.words, x, y))
+				continue;
+			unsigned long long k = order_key(fd.clean[(long long)y * fd.w + x]);
+			below += (k & used) == prefix && !(k & flag);
+		}
+		below = warp_sum_int(below);
+		used |= flag;
+		if (rank >= below) {
+			prefix |= flag;
+			rank -= below;
+		}
+	}
+	return order_value(prefix);
+}
+
+// Reference src/replace.cuh:111-153 over a compacted target list, one warp per
+// target: the median of the donors in the clipped (2r+1)^2 window, r = 2, 3,
+// ... until a donor exists.  In hole mode (initial fill) a frame runs when it
+// has finite donors; otherwise when its last pass flagged new pixels.
+__global__ void __launch_bounds__(256)
+replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
+	const uint2 *__restrict__ list, const unsigned long long *count, int hole_mode)
+{
+	const int lane = threadIdx.x & 31;
+	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	const long long n = (long long)*count;
+	for (long long e = gw; e < n; e += nw) {
+		const uint2 t = list[e];
+		const FrameState &st = state[t.x];
+		if (hole_mode ? !st.finite : !st.replace)
+			continue;
+		const FrameDesc &fd = frames[t.x];
+		const int w = fd.w, h = fd.h, words = fd.words;
+		const int x = (int)(t.y % (unsigned)w), y = (int)(t.y / (unsigned)w);
+		const uint32_t *don = plane_ptr(fd, P_DONOR), *crm = plane_ptr(fd, P_CRMASK);
+		const int limit = max(w, h);
+		for (int r = 2; r <= limit; ++r) {
+			Window win = {max(0, x - r), min(w - 1, x + r), max(0, y - r), min(h - 1, y + r)};
+			const int ww = win.x1 - win.x0 + 1, area = ww * (win.y1 - win.y0 + 1);
+			double lo, hi;
+			int nd;
+			if (area <= 32) {
+				bool d = false;
+				double v = INFINITY;
+				if (lane < area) {
+					int cx = win.x0 + lane % ww, cy = win.y0 + lane / ww;
+					d = donor_at(don, crm, words, cx, cy);
+					if (d)
+						v = fd.clean[(long long)cy * w + cx];
+				}
+				nd = __popc(__ballot_sync(0xffffffffu, d));
+				if (!nd)
+					continue;
+				v = bitonic32(v);
+				lo = __shfl_sync(0xffffffffu, v, (nd - 1) / 2);
+				hi = __shfl_sync(0xffffffffu, v, nd / 2);
+			} else {
+				int cnt = 0;
+				for (int pos = lane; pos < area; pos += 32)
+					cnt += donor_at(don, crm, words, win.x0 + pos % ww, win.y0 + pos / ww);
+				nd = warp_sum_int(cnt);
+				if (!nd)
+					continue;
+				lo = select_rank(fd, don, crm, win, (nd - 1) / 2);
+				hi = nd % 2 ? lo : select_rank(fd, don, crm, win, nd / 2);
+			}
+			if (lane == 0)
+				fd.clean[t.y] = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
+			break;
+		}
+	}
+}
+
+// Reference src/image.cuh:50-70, in place: clean -= bg, non-finite inputs
+// restored bit for bit, uint8 mask from the bit plane.
+__global__ void __launch_bounds__(256)
+restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ rows, int nrows)
+{
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int r = gw; r < nrows; r += nw) {
+		const int2 item = rows[r];
+		const FrameDesc &fd = frames[item.x];
+		const int w = fd.w, y = item.y, words = fd.words;
+		const uint32_t *hole = plane_ptr(fd, P_HOLE) + (long long)y * words;
+		const uint32_t *crm = plane_ptr(fd, P_CRMASK) + (long long)y * words;
+		const long long rowpix = (long long)y * w;
+		for (int x = lane; x < w; x += 32) {
+			const long long i = rowpix + x;
+			const uint32_t hb = hole[x >> 5], cb = crm[x >> 5];
+			double v = fd.clean[i];
+			if (fd.has_bg)
+				v += -1 * (fd.bg_map ? fd.bg_map[i] : fd.bg);
+			if ((hb >> (x & 31)) & 1u)
+				v = fd.data[i];
+			fd.clean[i] = v;
+			fd.mask_out[i] = (cb >> (x & 31)) & 1u;
+		}
+	}
+}
+
+// maxiter == 0 (reference src/image.cuh:72-92): background round trip only.
+__global__ void __launch_bounds__(256)
+copy_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ rows, int nrows)
+{
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int r = gw; r < nrows; r += nw) {
+		const int2 item = rows[r];
+		const FrameDesc &fd = frames[item.x];
+		const long long rowpix = (long long)item.y * fd.w;
+		for (int x = lane; x < fd.w; x += 32) {
+			const long long i = rowpix + x;
+			const double d = fd.data[i];
+			double v = isfinite(d) ? d : 0;
+			if (fd.has_bg) {
+				double bg = fd.bg_map ? fd.bg_map[i] : fd.bg;
+				v += 1 * bg;
+				v += -1 * bg;
+			}
+			fd.clean[i] = isfinite(d) ? v : d;
+			fd.mask_out[i] = 0;
+		}
+	}
+}
+
+} // namespace cb

@@ -1,0 +1,111 @@
+/*
+ * cusmic_b200 extensions to the reference C ABI (cusmic.h).
+ *
+ * The reference batch call (src/cusmic.h:80-85) accepts only same-shaped
+ * frames with batch-wide scalar calibration, allocates scratch on every call
+ * and synchronises the host once per iteration (src/cleaner.cuh:128-142).
+ * These entry points add what a B200 deployment needs on top of it:
+ *
+ *   - ragged batches with per-frame scalar gain / read noise / background,
+ *     run as one persistent launch over a tile work list;
+ *   - plans: a workspace, tile list and captured CUDA graph of the whole
+ *     maxiter loop (with its early exit as a device-side while node), reused
+ *     across executions;
+ *   - the adjoint of the cleaned pixels with the detection mask frozen.
+ *
+ * All pointers of a call belong to the caller's current device.  Status codes
+ * and message conventions are those of cusmic.h.
+ */
+#ifndef CUSMIC_B200_H
+#define CUSMIC_B200_H
+
+#include "cusmic.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-frame scalar calibration of a ragged batch.  A NaN gain or read noise
+ * falls back to the options' value; a NaN background means none for that
+ * frame.  Maps in the frame's cusmic_image still override these scalars.
+ * No counterpart in the reference, whose scalars are batch-wide
+ * (src/cusmic.h:45-51). */
+struct cusmic_frame_scalars {
+	double gain, readnoise, background;
+};
+
+/* Ragged batch of 1..65535 device frames of any shapes.  Frame f's outputs
+ * start at offset sum_{g<f} width_g * height_g of clean and mask.  scalars
+ * may be NULL.  Synchronises before returning, like remove_cosmics_device.
+ * Generalises remove_cosmics_batch_device (reference src/api.cu:184-192). */
+int
+cusmic_ragged_batch_device(const struct cusmic_image *ims, size_t nf,
+	const struct cusmic_options *options, const struct cusmic_frame_scalars *scalars,
+	double *clean, uint8_t *mask, void *stream, char *msg, size_t message_size);
+
+typedef struct cusmic_plan cusmic_plan;
+
+/* Plan flags. */
+enum cusmic_plan_flags {
+	CUSMIC_PLAN_GRAPH = 1, /* capture the maxiter loop into one CUDA graph */
+	CUSMIC_PLAN_KEEP = 2   /* keep masks and target lists for cusmic_plan_backward */
+};
+
+/* Create a plan for a fixed batch (shapes, maps present or absent, options)
+ * bound to the given device buffers.  Allocates the workspace once.  No
+ * counterpart in the reference (its scratch is per call, src/cleaner.cuh:39-61). */
+int
+cusmic_plan_create(cusmic_plan **plan, const struct cusmic_image *ims, size_t nf,
+	const struct cusmic_options *options, const struct cusmic_frame_scalars *scalars,
+	double *clean, uint8_t *mask, int flags, char *msg, size_t message_size);
+
+/* Rebind the plan to new device buffers of the same shapes and map layout
+ * (pointers only; the next execution reads the new descriptors). */
+int
+cusmic_plan_bind(cusmic_plan *plan, const struct cusmic_image *ims, double *clean,
+	uint8_t *mask, char *msg, size_t message_size);
+
+/* Enqueue one cleaning of the bound batch on stream; does not synchronise. */
+int
+cusmic_plan_execute(cusmic_plan *plan, void *stream, char *msg, size_t message_size);
+
+/* Wait for the plan's last execution and report its status ("no finite
+ * replacement donors" is CUSMIC_INVALID, as in the reference). */
+int
+cusmic_plan_wait(cusmic_plan *plan, char *msg, size_t message_size);
+
+/* Detection passes run per frame by the last execution (nf ints, host). */
+int
+cusmic_plan_passes(cusmic_plan *plan, int *passes);
+
+/* Execute the plan once without its graph, with a CUDA event recorded on
+ * stream after every kernel, then synchronise.  ms[k] and launches[k] receive
+ * the summed duration and launch count of kernel kind k for k in 0..8:
+ * init, prepare, hole fill, detect, grow/update, control, replace, restore,
+ * zero-iteration copy (kinds >= 9).  A timing aid; no counterpart in the
+ * reference. */
+int
+cusmic_plan_profile(cusmic_plan *plan, void *stream, double *ms, int *launches, int kinds,
+	char *msg, size_t message_size);
+
+/* Adjoint of the last execution with its detection mask frozen: given
+ * grad_clean = dL/d(clean) (device, laid out like the outputs) writes
+ * grad_data = dL/d(data), and, when not NULL, grad_background = dL/d(background):
+ * one value per frame for scalar backgrounds, or a full map laid out like the
+ * outputs when the batch used background maps.  Each replaced pixel sends its
+ * gradient to the donor its replacement median selected (half to each of the
+ * two central donors for an even donor count, ties broken by lowest linear
+ * index); unflagged and non-finite pixels pass it straight through.  Needs a
+ * plan created with CUSMIC_PLAN_KEEP.  Enqueued on stream; synchronises.
+ * No counterpart in the reference. */
+int
+cusmic_plan_backward(cusmic_plan *plan, const double *grad_clean, double *grad_data,
+	double *grad_background, void *stream, char *msg, size_t message_size);
+
+void
+cusmic_plan_destroy(cusmic_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

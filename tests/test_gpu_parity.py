@@ -1,0 +1,316 @@
+"""GPU parity of libcusmic_b200.so against the CPU oracle, the reference's golden
+fixture, the reference's known answers and (when built) the reference's own
+CUDA library.  Pixels and masks must be bit-identical.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from tests import cabi
+from tests.conftest import assert_bits_equal
+
+pytestmark = pytest.mark.gpu
+
+MODES = ("mirror", "reflect", "nearest", "wrap", "constant")
+SETTINGS = dict(contrast=3.0, cr_threshold=5.0, neighbor_threshold=3.0)
+
+
+def small_scene(seed, h, w, *, holes=0.0, masked=0.0, rays=None, sky=100.0):
+    rng = np.random.default_rng(seed)
+    data = sky + rng.normal(0, math.sqrt(sky + 9), (h, w))
+    yy, xx = np.mgrid[0:h, 0:w]
+    for _ in range(max(1, h * w // 400)):
+        cy, cx = rng.uniform(0, h), rng.uniform(0, w)
+        data += rng.uniform(50, 2000) * np.exp(-((yy - cy) ** 2 + (xx - cx) ** 2) / 2.0)
+    for _ in range(rays if rays is not None else max(1, h * w // 150)):
+        y, x = rng.integers(0, h), rng.integers(0, w)
+        a = rng.uniform(200, 5000)
+        data[y, x] += a
+        if rng.random() < 0.4 and x + 1 < w:
+            data[y, x + 1] += a / 2
+    if holes:
+        data[rng.random((h, w)) < holes] = np.nan
+    mask = rng.random((h, w)) < masked if masked else None
+    return data, mask
+
+
+def check_against_oracle(oracle, frames, opts_kw, *, ragged=False):
+    fr = cabi.Frames(frames)
+    opts = cabi.options(**opts_kw)
+    if ragged:
+        st, msg = cabi.run_ragged(fr, opts)
+    else:
+        st, msg = cabi.run_batch(cabi._native.lib(), fr, opts)
+    settings = {k: v for k, v in opts_kw.items() if k in
+                ("contrast", "cr_threshold", "neighbor_threshold", "maxiter", "border")}
+    want = []
+    for f in frames:
+        try:
+            want.append(cabi.oracle_frame(oracle, f, **settings))
+        except oracle.OracleError as e:
+            want.append(e)
+    if any(isinstance(wt, Exception) for wt in want):
+        assert st == cabi._native.CUSMIC_INVALID and "no finite replacement donors" in msg
+        return fr
+    assert st == 0, msg
+    for (want_clean, want_mask, _), (clean, mask) in zip(want, fr.outputs()):
+        np.testing.assert_array_equal(mask, want_mask)
+        assert_bits_equal(clean, want_clean)
+    return fr
+
+
+def test_golden_fixture_python_api(cuda, golden):
+    from cusmic_b200 import remove_cosmics
+    data = cuda.from_numpy(golden["data"]).cuda()
+    error = cuda.from_numpy(golden["error"]).cuda()
+    cleaned, mask = remove_cosmics(data, error=error, **golden["settings"])
+    np.testing.assert_array_equal(mask.cpu().numpy(), golden["mask"])
+    assert_bits_equal(cleaned.cpu().numpy(), golden["cleaned"])
+
+
+def test_golden_fixture_host_api(cuda, golden):
+    """The host entry point, as reference test/test_reference.c:25-120 calls it."""
+    from cusmic_b200 import _native
+    data = np.ascontiguousarray(golden["data"])
+    error = np.ascontiguousarray(golden["error"])
+    im = _native.Image(data.ctypes.data, error.ctypes.data, None, None, None, None, 512, 512)
+    o = cabi.options(contrast=1.0, cr_threshold=5.0, neighbor_threshold=5.0)
+    clean = np.empty_like(data)
+    mask = np.empty(data.shape, np.uint8)
+    msg = ctypes.create_string_buffer(256)
+    st = _native.lib().remove_cosmics(ctypes.byref(im), ctypes.byref(o), clean.ctypes.data,
+                                      mask.ctypes.data, msg, 256)
+    assert st == 0, msg.value
+    np.testing.assert_array_equal(mask.astype(bool), golden["mask"])
+    assert_bits_equal(clean, golden["cleaned"])
+
+
+def test_plain_512_noise_model(cuda, oracle):
+    from cusmic_b200 import scenes
+    sc = scenes.plain_512()
+    f = sc.frames[0]
+    frames = [dict(data=f.data)]
+    check_against_oracle(oracle, frames, dict(SETTINGS, gain=2.0, readnoise=5.0, background=0.0))
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("path", ("error", "model"))
+def test_modes_masks_holes_background(cuda, oracle, mode, path):
+    data, mask = small_scene(MODES.index(mode) * 2 + (path == "model"), 70, 93, holes=0.01, masked=0.02)
+    rng = np.random.default_rng(7)
+    frame = dict(data=data, mask=mask, background=rng.uniform(0, 50, data.shape))
+    if path == "error":
+        frame["error"] = np.sqrt(np.abs(np.nan_to_num(data)) + 9)
+    else:
+        frame["gain"] = rng.uniform(0.8, 1.2, data.shape)
+        frame["readnoise"] = 3.0
+    check_against_oracle(oracle, [frame], dict(SETTINGS, border=mode,
+                                               readnoise=frame.get("readnoise", 0.0)))
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("shape", ((1, 1), (1, 9), (9, 1), (2, 2), (3, 5), (5, 3), (2, 40),
+                                   (40, 2), (33, 31), (64, 65)))
+def test_small_shapes(cuda, oracle, mode, shape):
+    data, _ = small_scene(shape[0] * 100 + shape[1], *shape, rays=max(1, shape[0] * shape[1] // 30))
+    frame = dict(data=data, gain=1.0, readnoise=3.0)
+    check_against_oracle(oracle, [frame], dict(SETTINGS, border=mode, gain=1.0, readnoise=3.0))
+
+
+@pytest.mark.parametrize("thresholds", ((0.0, 0.0, 0.0), (1.0, 5.0, 5.0), (3.0, 2.0, 0.5)))
+def test_thresholds(cuda, oracle, thresholds):
+    contrast, cr, nb = thresholds
+    data, _ = small_scene(11, 48, 64)
+    frame = dict(data=data, error=np.full(data.shape, 10.0))
+    check_against_oracle(oracle, [frame], dict(contrast=contrast, cr_threshold=cr,
+                                               neighbor_threshold=nb))
+
+
+def test_ragged_batch_per_frame_scalars(cuda, oracle):
+    frames = []
+    rng = np.random.default_rng(5)
+    for i, (h, w) in enumerate(((40, 70), (128, 33), (17, 200), (96, 96), (5, 7))):
+        data, mask = small_scene(20 + i, h, w, holes=0.005, masked=0.01)
+        frames.append(dict(data=data, mask=mask, gain=float(rng.uniform(1, 4)),
+                           readnoise=float(rng.uniform(2, 10)),
+                           background=float(rng.uniform(0, 200))))
+    check_against_oracle(oracle, frames, dict(SETTINGS), ragged=True)
+
+
+def test_batch_matches_single_calls(cuda):
+    """reference test/test_batch.cu:46-169: a 3-frame 9x9 batch equals single calls."""
+    frames = []
+    for f in range(3):
+        d = np.full((9, 9), 10.0 + f)
+        d[4 + f % 2, 4 + f // 2] = 1000 + 100 * f
+        frames.append(dict(data=d, error=np.ones((9, 9))))
+    lib = cabi._native.lib()
+    batch = cabi.Frames(frames)
+    assert cabi.run_batch(lib, batch, cabi.options())[0] == 0
+    outs = batch.outputs()
+    for f, fr in enumerate(frames):
+        one = cabi.Frames([fr])
+        assert cabi.run_batch(lib, one, cabi.options())[0] == 0
+        (c1, m1), = one.outputs()
+        assert_bits_equal(outs[f][0], c1)
+        np.testing.assert_array_equal(outs[f][1], m1)
+        assert m1[4 + f % 2, 4 + f // 2]
+
+
+def test_graph_plan_matches_plain(cuda, oracle):
+    frames = []
+    for i, (h, w) in enumerate(((300, 257), (64, 512), (129, 129))):
+        data, mask = small_scene(40 + i, h, w, holes=0.002, masked=0.01)
+        frames.append(dict(data=data, mask=mask, gain=2.0, readnoise=5.0, background=10.0 * i))
+    opts = cabi.options(**SETTINGS)
+    want = []
+    for f in frames:
+        c, m, p = cabi.oracle_frame(oracle, f, **SETTINGS)
+        want.append((c, m, p))
+    for flags in (0, cabi._native.PLAN_GRAPH):
+        fr = cabi.Frames(frames)
+        plan = cabi.Plan(fr, opts, flags)
+        try:
+            for _ in range(2):
+                st, msg = plan.run()
+                assert st == 0, msg
+                for (c, m), (wc, wm, _) in zip(fr.outputs(), want):
+                    np.testing.assert_array_equal(m, wm)
+                    assert_bits_equal(c, wc)
+                assert plan.passes() == [p for _, _, p in want]
+        finally:
+            plan.close()
+
+
+def test_reference_known_answers(cuda):
+    from cusmic_b200 import remove_cosmics
+    image = np.full((15, 15), 10.0)
+    image[5:10, 5:10] = 1000
+    cleaned, mask = remove_cosmics(image, **SETTINGS, error=np.ones_like(image))
+    np.testing.assert_array_equal(cleaned.cpu().numpy(), 10)
+    np.testing.assert_array_equal(mask.cpu().numpy(), image == 1000)
+
+    image = np.full((3, 3), 0.1)
+    cleaned, mask = remove_cosmics(image, **SETTINGS, background=1e12, maxiter=0)
+    assert_bits_equal(cleaned.cpu().numpy(), (np.full((3, 3), 0.1) + 1e12) - 1e12)
+    assert not mask.any()
+
+    data = np.full((9, 9), 10.0)
+    data[2:7, 2:7] = np.nan
+    data[3, 3], data[3, 5], data[4, 4] = np.inf, -np.inf, 1000
+    data.view("uint64")[2, 2] = 0x7FF8000000000001
+    for maxiter in (0, 4):
+        clean, mask = remove_cosmics(data, **SETTINGS, error=np.ones_like(data), background=100,
+                                     maxiter=maxiter)
+        expected = data.copy()
+        if maxiter:
+            expected[4, 4] = 10
+        assert_bits_equal(clean.cpu().numpy(), expected)
+        assert int(mask.sum()) == bool(maxiter)
+    data[:] = np.nan
+    clean, mask = remove_cosmics(data, **SETTINGS, error=np.ones_like(data))
+    assert_bits_equal(clean.cpu().numpy(), data)
+    assert not mask.any()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_singleton_borders(cuda, mode):
+    """reference test/test_batch.cu:170-198 through the host entry point."""
+    from cusmic_b200 import _native
+    probe = np.where(np.arange(9) == 4, 1000.0, 10.0)
+    error = np.ones(9)
+    want = np.arange(9) == 4
+    if mode == "constant":
+        want |= np.isin(np.arange(9), (0, 1, 7, 8))
+    for w, h in ((9, 1), (1, 9)):
+        im = _native.Image(probe.ctypes.data, error.ctypes.data, None, None, None, None, w, h)
+        o = cabi.options(border=mode)
+        clean = np.empty(9)
+        mask = np.empty(9, np.uint8)
+        msg = ctypes.create_string_buffer(256)
+        assert _native.lib().remove_cosmics(ctypes.byref(im), ctypes.byref(o), clean.ctypes.data,
+                                            mask.ctypes.data, msg, 256) == 0, msg.value
+        np.testing.assert_array_equal(clean, 10)
+        np.testing.assert_array_equal(mask.astype(bool), want)
+
+
+def test_host_api_keeps_special_bits_and_outputs_on_failure(cuda):
+    """reference test/test_api.c:22-57."""
+    from cusmic_b200 import _native
+    data = np.array([1, -0.0, 3, 4])
+    data.view(np.uint64)[2] = 0x7FF8000000001234
+    before = data.copy()
+    im = _native.Image(data.ctypes.data, None, None, None, None, None, 2, 2)
+    o = cabi.options(maxiter=0)
+    clean = np.full(4, 9.0)
+    mask = np.full(4, 9, np.uint8)
+    msg = ctypes.create_string_buffer(128)
+    L = _native.lib()
+    assert L.remove_cosmics(ctypes.byref(im), ctypes.byref(o), clean.ctypes.data,
+                            mask.ctypes.data, msg, 128) == 0
+    assert_bits_equal(clean, before)
+    assert_bits_equal(data, before)
+    assert not mask.any()
+    o.cr_threshold = math.nan
+    clean[:] = 9
+    mask[:] = 9
+    assert L.remove_cosmics(ctypes.byref(im), ctypes.byref(o), clean.ctypes.data,
+                            mask.ctypes.data, msg, 128) == _native.CUSMIC_INVALID
+    assert (clean == 9).all() and (mask == 9).all()
+
+
+def test_no_donor_error(cuda):
+    from cusmic_b200 import remove_cosmics
+    data = np.full((7, 7), 10.0)
+    data[3, 3] = 1000
+    mask = np.ones((7, 7), bool)
+    mask[3, 3] = False
+    with pytest.raises(ValueError, match="no finite replacement donors"):
+        remove_cosmics(data, **SETTINGS, error=np.ones_like(data), mask=mask)
+
+
+def test_stream_handoff(cuda):
+    """reference test/test_streams.py:7-33 with torch streams and events."""
+    from cusmic_b200 import Cleaner, Image
+    torch = cuda
+    producer, consumer = torch.cuda.Stream(), torch.cuda.Stream()
+    data = torch.empty((9, 9), dtype=torch.float64, device="cuda")
+    error = torch.empty((9, 9), dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(producer):
+        torch.cuda._sleep(10_000_000)
+        data.fill_(10)
+        data[4, 4] = 1000
+        error.fill_(1)
+    ready = producer.record_event()
+    consumer.wait_event(ready)
+    with torch.cuda.stream(consumer):
+        clean, mask = Cleaner()(Image(data, error=error))
+    np.testing.assert_array_equal(clean.cpu().numpy(), 10)
+    assert int(mask.sum()) == 1
+
+
+@pytest.mark.parametrize("workload", ("plain_512", "stack_1024"))
+def test_reference_library_parity(cuda, workload):
+    """Bit parity with the reference's own CUDA library built for sm_100a."""
+    ref = cabi.reference_lib()
+    if ref is None:
+        pytest.skip("oracle/_ref/libcusmic_ref.so was not built")
+    from cusmic_b200 import scenes
+    if workload == "plain_512":
+        f = scenes.plain_512().frames[0]
+        frames = [dict(data=f.data)]
+        kw = dict(SETTINGS, gain=2.0, readnoise=5.0, background=0.0)
+    else:
+        sc = scenes.stack_2048(frames=2, size=1024)
+        frames = [dict(data=f.data, error=sc.error, mask=sc.mask) for f in sc.frames]
+        kw = dict(SETTINGS)
+    mine, theirs = cabi.Frames(frames), cabi.Frames(frames)
+    assert cabi.run_batch(cabi._native.lib(), mine, cabi.options(**kw))[0] == 0
+    st, msg = cabi.run_batch(ref, theirs, cabi.options(**kw))
+    assert st == 0, msg
+    for (c1, m1), (c2, m2) in zip(mine.outputs(), theirs.outputs()):
+        np.testing.assert_array_equal(m1, m2)
+        assert_bits_equal(c1, c2)
