@@ -21,8 +21,8 @@ EXPORTS = (
     "cusmic_plan_create", "cusmic_plan_bind", "cusmic_plan_execute", "cusmic_plan_wait",
     "cusmic_plan_passes", "cusmic_plan_profile", "cusmic_plan_backward", "cusmic_plan_destroy",
 )
-KERNEL_KINDS = ("init", "prepare", "fill", "detect", "grow", "control", "replace", "restore",
-                "copy")
+KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
+                "replace", "restore", "copy")
 
 
 class Image(ctypes.Structure):

@@ -97,6 +97,7 @@ struct FrameState {
 struct Control {
 	unsigned long long n_targets; // length of the target list
 	unsigned long long n_holes;   // length of the hole list (front of the same buffer)
+	unsigned long long n_cand;    // this pass: pixels whose sig_raw can pass a threshold
 	int iter;                     // detection passes issued so far
 	int maxiter;
 	int any_active;

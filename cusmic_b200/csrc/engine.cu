@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "detect.cuh"
 #include "kernels.cuh"
+#include "backward.cuh"
 
 #include <climits>
 #include <cmath>
@@ -42,9 +43,6 @@ static void check(cudaError_t e)
 		throw std::runtime_error(cudaGetErrorString(e));
 }
 
-constexpr int TILE_W = 32, TILE_H = 32, DETECT_THREADS = 256;
-using Tile = DetectTile<TILE_W, TILE_H>;
-#define DETECT_KERNEL detect_kernel<TILE_W, TILE_H, DETECT_THREADS>
 
 template <class T> struct DevBuf {
 	T *p = nullptr;
@@ -100,8 +98,10 @@ template <class T> struct PinBuf {
 struct Layout {
 	std::vector<FrameDesc> frames;
 	std::vector<long long> bit_off; // word offset of each frame's planes
-	std::vector<int4> tiles;
+	std::vector<int4> tiles; // sig_model_kernel tiles (noise-model frames)
+	std::vector<int4> strips; // sig_stream_kernel items (error-map frames)
 	std::vector<int2> rows;
+	std::vector<long long> offsets; // first output pixel of each frame
 	long long total_words = 0;
 	size_t total_px = 0;
 	DetectParams prm{};
@@ -109,7 +109,7 @@ struct Layout {
 };
 
 struct DeviceInfo {
-	int sms = 0, detect_blocks_per_sm = 0;
+	int sms = 0;
 };
 
 static DeviceInfo device_info(int dev)
@@ -120,15 +120,8 @@ static DeviceInfo device_info(int dev)
 	if ((int)cache.size() <= dev)
 		cache.resize(dev + 1);
 	DeviceInfo &d = cache[dev];
-	if (!d.sms) {
+	if (!d.sms)
 		check(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
-		check(cudaFuncSetAttribute(DETECT_KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			(int)sizeof(Tile)));
-		check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.detect_blocks_per_sm,
-			DETECT_KERNEL, DETECT_THREADS, sizeof(Tile)));
-		if (d.detect_blocks_per_sm < 1)
-			d.detect_blocks_per_sm = 1;
-	}
 	return d;
 }
 
@@ -140,7 +133,11 @@ struct Workspace {
 	DevBuf<int2> rows;
 	DevBuf<uint32_t> bits;
 	DevBuf<uint2> targets;
+	DevBuf<uint2> cands;
+	DevBuf<Seed> seeds;
+	DevBuf<int4> strips;
 	DevBuf<Control> ctl;
+	DevBuf<long long> offsets;
 	PinBuf<unsigned char> stage;
 	PinBuf<FrameState> hstate;
 	// Host-API staging of inputs and outputs.
@@ -245,6 +242,7 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 	L.prm.cr = o.cr_threshold;
 	L.prm.nb = o.neighbor_threshold;
 	L.prm.tmin = std::fmin(o.cr_threshold, o.neighbor_threshold);
+	L.prm.tloose = L.prm.tmin * (1 - 1e-12);
 	L.prm.mode = o.border;
 	L.frames.resize(nf);
 	L.bit_off.resize(nf);
@@ -272,13 +270,20 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		d.has_bg = im.background != nullptr || !std::isnan(s.bg);
 		d.bits = nullptr;
 		L.bit_off[f] = words;
+		L.offsets.push_back((long long)px);
 		words += (long long)N_PLANES * d.plane;
 		px += (size_t)d.w * d.h;
 		for (int y = 0; y < d.h; ++y)
 			L.rows.push_back(make_int2((int)f, y));
-		for (int ty = 0; ty < d.h; ty += TILE_H)
-			for (int tx = 0; tx < d.w; tx += TILE_W)
-				L.tiles.push_back(make_int4((int)f, tx, ty, 0));
+		if (d.error) {
+			for (int ty = 0; ty < d.h; ty += STREAM_ROWS)
+				for (int tx = 0; tx < d.w; tx += 32)
+					L.strips.push_back(make_int4((int)f, tx, ty, 0));
+		} else {
+			for (int ty = 0; ty < d.h; ty += MTILE)
+				for (int tx = 0; tx < d.w; tx += MTILE)
+					L.tiles.push_back(make_int4((int)f, tx, ty, 0));
+		}
 	}
 	L.total_px = px;
 	L.total_words = words;
@@ -299,27 +304,40 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	ws.frames.ensure(nf);
 	ws.state.ensure(nf);
 	ws.tiles.ensure(L.tiles.size() ? L.tiles.size() : 1);
+	ws.strips.ensure(L.strips.size() ? L.strips.size() : 1);
 	ws.rows.ensure(L.rows.size());
 	ws.ctl.ensure(1);
+	ws.offsets.ensure(nf);
 	if (L.maxiter) {
 		ws.bits.ensure((size_t)L.total_words);
 		ws.targets.ensure(L.total_px);
+		ws.cands.ensure(L.total_px);
+		ws.seeds.ensure(L.total_px);
 	}
 	for (size_t f = 0; f < nf; ++f)
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
 	size_t bytes_f = nf * sizeof(FrameDesc), bytes_t = L.tiles.size() * sizeof(int4);
-	size_t bytes_r = L.rows.size() * sizeof(int2);
-	ws.stage.ensure(bytes_f + bytes_t + bytes_r);
+	size_t bytes_s = L.strips.size() * sizeof(int4), bytes_r = L.rows.size() * sizeof(int2);
+	ws.stage.ensure(bytes_f + bytes_t + bytes_s + bytes_r);
 	// The previous call using this workspace synchronised before returning,
 	// so the staging buffer is free.
-	std::memcpy(ws.stage.p, L.frames.data(), bytes_f);
-	std::memcpy(ws.stage.p + bytes_f, L.tiles.data(), bytes_t);
-	std::memcpy(ws.stage.p + bytes_f + bytes_t, L.rows.data(), bytes_r);
-	check(cudaMemcpyAsync(ws.frames.p, ws.stage.p, bytes_f, cudaMemcpyHostToDevice, s));
+	unsigned char *st = ws.stage.p;
+	std::memcpy(st, L.frames.data(), bytes_f);
+	std::memcpy(st + bytes_f, L.tiles.data(), bytes_t);
+	std::memcpy(st + bytes_f + bytes_t, L.strips.data(), bytes_s);
+	std::memcpy(st + bytes_f + bytes_t + bytes_s, L.rows.data(), bytes_r);
+	check(cudaMemcpyAsync(ws.frames.p, st, bytes_f, cudaMemcpyHostToDevice, s));
 	if (bytes_t)
-		check(cudaMemcpyAsync(ws.tiles.p, ws.stage.p + bytes_f, bytes_t, cudaMemcpyHostToDevice, s));
-	check(cudaMemcpyAsync(ws.rows.p, ws.stage.p + bytes_f + bytes_t, bytes_r,
+		check(cudaMemcpyAsync(ws.tiles.p, st + bytes_f, bytes_t, cudaMemcpyHostToDevice, s));
+	if (bytes_s)
+		check(cudaMemcpyAsync(ws.strips.p, st + bytes_f + bytes_t, bytes_s,
+			cudaMemcpyHostToDevice, s));
+	check(cudaMemcpyAsync(ws.rows.p, st + bytes_f + bytes_t + bytes_s, bytes_r,
 		cudaMemcpyHostToDevice, s));
+	// Offsets are only read by the adjoint; a synchronous copy is fine.
+	check(cudaStreamSynchronize(s));
+	check(cudaMemcpy(ws.offsets.p, L.offsets.data(), nf * sizeof(long long),
+		cudaMemcpyHostToDevice));
 }
 
 struct GraphLoop {
@@ -328,8 +346,8 @@ struct GraphLoop {
 };
 
 // Kernel kinds reported by cusmic_plan_profile().
-enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_DETECT, K_GROW, K_CONTROL, K_REPLACE, K_RESTORE,
-	K_COPY, K_KINDS };
+enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_SIGRAW, K_CAND, K_SEED, K_GROW, K_CONTROL,
+	K_REPLACE, K_RESTORE, K_COPY, K_KINDS };
 
 // Optional CUDA-event timer: an event after every launch on the launching
 // stream, so each kernel's duration is the gap to the previous event.
@@ -366,13 +384,24 @@ static inline void mark(Recorder *r, int kind)
 static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
 	const GraphLoop &gl, Recorder *rec = nullptr)
 {
-	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size(), ntiles = (int)L.tiles.size();
-	int dblocks = di.sms * di.detect_blocks_per_sm;
-	if (dblocks > ntiles)
-		dblocks = ntiles;
-	DETECT_KERNEL<<<dblocks, DETECT_THREADS, sizeof(Tile), s>>>(ws.frames.p, ws.state.p,
-		ws.tiles.p, ntiles, L.prm);
-	mark(rec, K_DETECT);
+	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
+	const int ntiles = (int)L.tiles.size(), nstrips = (int)L.strips.size();
+	if (nstrips) {
+		int blocks = (nstrips + 7) / 8, cap = di.sms * 8;
+		sig_stream_kernel<<<blocks < cap ? blocks : cap, 256, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.strips.p, nstrips, L.prm, ws.ctl.p, ws.cands.p);
+	}
+	if (ntiles) {
+		int cap = di.sms * 8;
+		sig_model_kernel<<<ntiles < cap ? ntiles : cap, 256, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.tiles.p, ntiles, L.prm, ws.ctl.p, ws.cands.p);
+	}
+	mark(rec, K_SIGRAW);
+	candidate_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
+		ws.seeds.p);
+	mark(rec, K_CAND);
+	seed_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p);
+	mark(rec, K_SEED);
 	grow_update_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.rows.p, nrows, ws.targets.p, ws.ctl.p);
 	mark(rec, K_GROW);
@@ -822,6 +851,41 @@ extern "C" int cusmic_plan_profile(cusmic_plan *p, void *stream, double *ms, int
 extern "C" int cusmic_plan_backward(cusmic_plan *p, const double *grad_clean, double *grad_data,
 	double *grad_background, void *stream, char *msg, size_t len)
 {
-	(void)p, (void)grad_clean, (void)grad_data, (void)grad_background, (void)stream;
-	return guarded([&] { throw InvalidArgument("backward is not available in this build"); }, msg, len);
+	return guarded([&] {
+		if (!p || !grad_clean || !grad_data)
+			throw InvalidArgument("invalid plan or gradient buffers");
+		if (!p->executed)
+			throw InvalidArgument("plan has not been executed");
+		check(cudaStreamSynchronize(p->last));
+		const size_t nf = p->L.frames.size();
+		for (size_t f = 0; f < nf; ++f) {
+			const FrameState &st = p->ws.hstate.p[f];
+			if (st.error || (st.holes && st.allowed && !st.finite))
+				throw InvalidArgument("no finite replacement donors");
+		}
+		bool map_mode = false;
+		for (const FrameDesc &d : p->L.frames)
+			map_mode |= d.bg_map != nullptr;
+		cudaStream_t s = (cudaStream_t)stream;
+		const Layout &L = p->L;
+		const int nrows = (int)L.rows.size();
+		if (grad_background && !map_mode)
+			check(cudaMemsetAsync(grad_background, 0, nf * sizeof(double), s));
+		if (!L.maxiter) {
+			// Zero iterations: out = (x + bg) - bg everywhere, an identity.
+			check(cudaMemcpyAsync(grad_data, grad_clean, L.total_px * sizeof(double),
+				cudaMemcpyDeviceToDevice, s));
+			if (grad_background && map_mode)
+				check(cudaMemsetAsync(grad_background, 0, L.total_px * sizeof(double), s));
+		} else {
+			bwd_dense_kernel<<<grid_for_rows(p->di, nrows), 256, 0, s>>>(p->ws.frames.p,
+				p->ws.rows.p, nrows, grad_clean, grad_data, map_mode ? grad_background : nullptr,
+				p->ws.offsets.p);
+			bwd_scatter_kernel<<<p->di.sms * 8, 256, 0, s>>>(p->ws.frames.p, p->ws.targets.p,
+				&p->ws.ctl.p->n_targets, p->ws.offsets.p, grad_clean, grad_data,
+				map_mode ? grad_background : nullptr, map_mode ? nullptr : grad_background);
+		}
+		check(cudaGetLastError());
+		check(cudaStreamSynchronize(s));
+	}, msg, len);
 }

@@ -63,7 +63,11 @@ __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter
 
 // Reference src/image.cuh:24-48: holes, exclusions, clean = data (+ bg), the
 // static donor plane (the reference's is_donor with an empty mask), counts,
-// and the hole list for the initial fill (src/cleaner.cuh:78-100).
+// and the hole list for the initial fill (src/cleaner.cuh:78-100).  A warp
+// loads ROW_UNROLL chunks of 32 pixels before using them, so enough bytes are
+// in flight per SM to approach the HBM bandwidth.
+constexpr int ROW_UNROLL = 4;
+
 __global__ void __launch_bounds__(256)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
 	int nrows, uint2 *holes_out, Control *ctl)
@@ -76,36 +80,56 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 		const int w = fd.w, y = item.y, words = fd.words;
 		const long long rowpix = (long long)y * w, roww = (long long)y * words;
 		int holes = 0, allowed = 0, finite = 0;
-		for (int x0 = 0; x0 < w; x0 += 32) {
-			const int x = x0 + lane;
-			const bool valid = x < w;
-			const long long i = rowpix + x;
-			bool hole = false, ok = false, donor = false;
-			if (valid) {
-				double d = fd.data[i];
-				hole = !isfinite(d);
-				ok = !hole && !(fd.mask && fd.mask[i]);
-				double c = hole ? 0 : d;
-				if (fd.has_bg)
-					c += 1 * (fd.bg_map ? fd.bg_map[i] : fd.bg);
-				fd.clean[i] = c;
-				donor = ok && isfinite(c);
+		for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
+			double d[ROW_UNROLL], bg[ROW_UNROLL];
+			bool m[ROW_UNROLL];
+#pragma unroll
+			for (int u = 0; u < ROW_UNROLL; ++u) {
+				const int x = xb + 32 * u + lane;
+				d[u] = 0;
+				bg[u] = fd.bg;
+				m[u] = false;
+				if (x < w) {
+					d[u] = fd.data[rowpix + x];
+					if (fd.mask)
+						m[u] = fd.mask[rowpix + x] != 0;
+					if (fd.bg_map)
+						bg[u] = fd.bg_map[rowpix + x];
+				}
 			}
-			const uint32_t hw = __ballot_sync(0xffffffffu, hole);
-			const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
-			const uint32_t dw = __ballot_sync(0xffffffffu, donor);
-			const uint32_t aw = __ballot_sync(0xffffffffu, ok);
-			if (lane < N_PLANES) {
-				uint32_t v = lane == P_HOLE ? hw : lane == P_EXCL ? ew : lane == P_DONOR ? dw : 0u;
-				plane_ptr(fd, lane)[roww + (x0 >> 5)] = v;
-			}
-			holes += __popc(hw);
-			allowed += __popc(aw);
-			finite += __popc(dw);
-			if (hw) {
-				unsigned long long base = warp_append(&ctl->n_holes, hole ? 1 : 0);
-				if (hole)
-					holes_out[base] = make_uint2((unsigned)item.x, (unsigned)i);
+#pragma unroll
+			for (int u = 0; u < ROW_UNROLL; ++u) {
+				const int x0 = xb + 32 * u;
+				if (x0 >= w)
+					break; // warp-uniform
+				const int x = x0 + lane;
+				const bool valid = x < w;
+				bool hole = false, ok = false, donor = false;
+				if (valid) {
+					hole = !isfinite(d[u]);
+					ok = !hole && !m[u];
+					double c = hole ? 0 : d[u];
+					if (fd.has_bg)
+						c += 1 * bg[u];
+					fd.clean[rowpix + x] = c;
+					donor = ok && isfinite(c);
+				}
+				const uint32_t hw = __ballot_sync(0xffffffffu, hole);
+				const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
+				const uint32_t dw = __ballot_sync(0xffffffffu, donor);
+				const uint32_t aw = __ballot_sync(0xffffffffu, ok);
+				if (lane < N_PLANES) {
+					uint32_t v = lane == P_HOLE ? hw : lane == P_EXCL ? ew : lane == P_DONOR ? dw : 0u;
+					plane_ptr(fd, lane)[roww + (x0 >> 5)] = v;
+				}
+				holes += __popc(hw);
+				allowed += __popc(aw);
+				finite += __popc(dw);
+				if (hw) {
+					unsigned long long base = warp_append(&ctl->n_holes, hole ? 1 : 0);
+					if (hole)
+						holes_out[base] = make_uint2((unsigned)item.x, (unsigned)(rowpix + x));
+				}
 			}
 		}
 		if (lane == 0) {
@@ -234,6 +258,7 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 	if (threadIdx.x == 0) {
 		int it = ++ctl->iter;
 		ctl->any_active = any;
+		ctl->n_cand = 0;
 		if (use_handle)
 			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
 	}
@@ -420,16 +445,36 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 		const uint32_t *hole = plane_ptr(fd, P_HOLE) + (long long)y * words;
 		const uint32_t *crm = plane_ptr(fd, P_CRMASK) + (long long)y * words;
 		const long long rowpix = (long long)y * w;
-		for (int x = lane; x < w; x += 32) {
-			const long long i = rowpix + x;
-			const uint32_t hb = hole[x >> 5], cb = crm[x >> 5];
-			double v = fd.clean[i];
-			if (fd.has_bg)
-				v += -1 * (fd.bg_map ? fd.bg_map[i] : fd.bg);
-			if ((hb >> (x & 31)) & 1u)
-				v = fd.data[i];
-			fd.clean[i] = v;
-			fd.mask_out[i] = (cb >> (x & 31)) & 1u;
+		for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
+			double v[ROW_UNROLL], bg[ROW_UNROLL];
+			uint32_t hb[ROW_UNROLL], cb[ROW_UNROLL];
+#pragma unroll
+			for (int u = 0; u < ROW_UNROLL; ++u) {
+				const int x = xb + 32 * u + lane;
+				v[u] = 0;
+				bg[u] = fd.bg;
+				hb[u] = cb[u] = 0;
+				if (x < w) {
+					v[u] = fd.clean[rowpix + x];
+					hb[u] = hole[x >> 5];
+					cb[u] = crm[x >> 5];
+					if (fd.bg_map)
+						bg[u] = fd.bg_map[rowpix + x];
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < ROW_UNROLL; ++u) {
+				const int x = xb + 32 * u + lane;
+				if (x < w) {
+					double o = v[u];
+					if (fd.has_bg)
+						o += -1 * bg[u];
+					if ((hb[u] >> (x & 31)) & 1u)
+						o = fd.data[rowpix + x];
+					fd.clean[rowpix + x] = o;
+					fd.mask_out[rowpix + x] = (cb[u] >> (x & 31)) & 1u;
+				}
+			}
 		}
 	}
 }

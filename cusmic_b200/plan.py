@@ -183,6 +183,28 @@ class Plan:
         _native.raise_for(st, msg)
         return (dict(zip(_native.KERNEL_KINDS, ms)), dict(zip(_native.KERNEL_KINDS, launches)))
 
+    def backward(self, grad_clean, stream=None):
+        """Adjoint of the last execution with its mask frozen.
+
+        ``grad_clean`` is laid out like the outputs.  Returns (grad_data,
+        grad_background): the latter per frame (nf values) unless the batch has
+        background maps, then per pixel like the outputs.
+        """
+        g = grad_clean.to(device=self.batch.device, dtype=torch.float64).contiguous()
+        if g.numel() != self.batch.total:
+            raise ValueError("gradient must match the outputs")
+        gx = torch.empty_like(self.batch.clean)
+        if any(b is not None for b in self.batch.backgrounds):
+            gbg = torch.empty_like(self.batch.clean)
+        else:
+            gbg = torch.empty(len(self.batch.frames), dtype=torch.float64,
+                              device=self.batch.device)
+        msg = ctypes.create_string_buffer(256)
+        st = _native.lib().cusmic_plan_backward(self.handle, g.data_ptr(), gx.data_ptr(),
+                                                gbg.data_ptr(), self._stream(stream), msg, 256)
+        _native.raise_for(st, msg)
+        return gx, gbg
+
     def close(self):
         if self.handle:
             _native.lib().cusmic_plan_destroy(self.handle)

@@ -48,7 +48,7 @@ typedef struct cusmic_plan cusmic_plan;
 /* Plan flags. */
 enum cusmic_plan_flags {
 	CUSMIC_PLAN_GRAPH = 1, /* capture the maxiter loop into one CUDA graph */
-	CUSMIC_PLAN_KEEP = 2   /* keep masks and target lists for cusmic_plan_backward */
+	CUSMIC_PLAN_KEEP = 2   /* reserved: plans always keep their last mask for the adjoint */
 };
 
 /* Create a plan for a fixed batch (shapes, maps present or absent, options)
@@ -80,9 +80,10 @@ cusmic_plan_passes(cusmic_plan *plan, int *passes);
 
 /* Execute the plan once without its graph, with a CUDA event recorded on
  * stream after every kernel, then synchronise.  ms[k] and launches[k] receive
- * the summed duration and launch count of kernel kind k for k in 0..8:
- * init, prepare, hole fill, detect, grow/update, control, replace, restore,
- * zero-iteration copy (kinds >= 9).  A timing aid; no counterpart in the
+ * the summed duration and launch count of kernel kind k for k in 0..10:
+ * init, prepare, hole fill, sig_raw (dense detection), candidates (5 x 5
+ * medians), seeds (fine structure), grow/update, control, replace, restore,
+ * zero-iteration copy (kinds >= 11).  A timing aid; no counterpart in the
  * reference. */
 int
 cusmic_plan_profile(cusmic_plan *plan, void *stream, double *ms, int *launches, int kinds,
@@ -91,12 +92,13 @@ cusmic_plan_profile(cusmic_plan *plan, void *stream, double *ms, int *launches, 
 /* Adjoint of the last execution with its detection mask frozen: given
  * grad_clean = dL/d(clean) (device, laid out like the outputs) writes
  * grad_data = dL/d(data), and, when not NULL, grad_background = dL/d(background):
- * one value per frame for scalar backgrounds, or a full map laid out like the
- * outputs when the batch used background maps.  Each replaced pixel sends its
- * gradient to the donor its replacement median selected (half to each of the
- * two central donors for an even donor count, ties broken by lowest linear
- * index); unflagged and non-finite pixels pass it straight through.  Needs a
- * plan created with CUSMIC_PLAN_KEEP.  Enqueued on stream; synchronises.
+ * one value per frame when no frame has a background map (zero for frames
+ * without background), else a per-pixel map laid out like the outputs.  Each
+ * replaced pixel sends its gradient to the donor its replacement median
+ * selected (half to each of the two central donors for an even donor count;
+ * donors ordered by value, ties by lowest linear index); unflagged and
+ * non-finite pixels pass it straight through.  The selection is recomputed
+ * from the plan's kept mask, not stored.  Runs on stream; synchronises.
  * No counterpart in the reference. */
 int
 cusmic_plan_backward(cusmic_plan *plan, const double *grad_clean, double *grad_data,

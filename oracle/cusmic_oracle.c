@@ -10,7 +10,7 @@
  * Parity is pinned by the reference's own golden fixture
  * (test/data/{input,error,reference}.fits.gz, lacosmic 1.4.0 output, stored
  * as tests/golden/fixture_512.npz) and, on a GPU, by the reference library
- * itself compiled from src/api.cu (see oracle/build_ref.py).
+ * itself compiled from src/api.cu (see oracle/build.py).
  *
  * Every function cites the reference file:line it follows (paths relative to
  * the reference project root).  Arithmetic must be compiled with
@@ -469,4 +469,95 @@ void
 oracle_replace(double *clean, const uint8_t *crmask, const uint8_t *excluded, int w, int h)
 {
 	replace(clean, crmask, excluded, w, h);
+}
+
+/*
+ * Reference gradient of the cleaned pixels with a frozen mask, from CPU
+ * selection indices (the adjoint has no counterpart in the reference; this
+ * is its definition).  For the final mask `crmask` of a forward run:
+ *   - unflagged pixels pass grad straight through (non-finite ones too);
+ *   - a flagged pixel sends grad to the donor its final replacement median
+ *     selected (odd count), or half to each of the two central donors (even
+ *     count); donors are finite, unmasked, unflagged pixels of data + bg,
+ *     ordered by IEEE total order (src/replace.cuh:37-48), ties by lowest
+ *     linear index;
+ *   - with background, flagged pixels add -grad to their own background and
+ *     the donor weights to the donors' backgrounds (scalar background: the
+ *     per-target sum, which is zero).
+ * grad_bg_map may be NULL; *grad_bg_scalar accumulates the scalar case.
+ */
+void
+oracle_backward(const oracle_image *im, const oracle_options *o, const uint8_t *crmask,
+	const double *grad, double *grad_data, double *grad_bg_map, double *grad_bg_scalar)
+{
+	int w = (int)im->width, h = (int)im->height;
+	size_t n = (size_t)w * h;
+	int has_bg = im->background || !isnan(o->background);
+	double *pre = malloc(n * sizeof(double));
+	uint8_t *donor = malloc(n);
+	uint64_t *keys = malloc(n * sizeof(uint64_t));
+	int *idx = malloc(n * sizeof(int));
+	for (size_t i = 0; i < n; ++i) {
+		double d = im->data[i];
+		double c = isfinite(d) ? d : 0;
+		if (has_bg)
+			c += 1 * (im->background ? im->background[i] : o->background);
+		pre[i] = c;
+		int excluded = !isfinite(d) || (im->mask && im->mask[i]);
+		donor[i] = !crmask[i] && !excluded && isfinite(c);
+		grad_data[i] = crmask[i] ? 0.0 : grad[i];
+		if (grad_bg_map)
+			grad_bg_map[i] = crmask[i] ? -grad[i] : 0.0;
+	}
+	double scalar = 0;
+	int limit = w > h ? w : h;
+	for (size_t i = 0; i < n; ++i) {
+		if (!crmask[i])
+			continue;
+		int x = (int)(i % w), y = (int)(i / w);
+		for (int r = 2; r <= limit; ++r) {
+			int x0 = x - r < 0 ? 0 : x - r, x1 = x + r > w - 1 ? w - 1 : x + r;
+			int y0 = y - r < 0 ? 0 : y - r, y1 = y + r > h - 1 ? h - 1 : y + r;
+			int count = 0;
+			for (int yy = y0; yy <= y1; ++yy)
+				for (int xx = x0; xx <= x1; ++xx) {
+					size_t j = (size_t)yy * w + xx;
+					if (!donor[j])
+						continue;
+					/* insertion by (key, linear index); cells arrive in
+					 * increasing linear index, so a strict key test is stable */
+					uint64_t k = order_key(pre[j]);
+					int p = count++;
+					while (p > 0 && k < keys[p - 1]) {
+						keys[p] = keys[p - 1];
+						idx[p] = idx[p - 1];
+						--p;
+					}
+					keys[p] = k;
+					idx[p] = (int)j;
+				}
+			if (!count)
+				continue;
+			double g = grad[i];
+			int lo = idx[(count - 1) / 2], hi = idx[count / 2];
+			double wl = count % 2 ? g : g / 2, wh = count % 2 ? 0.0 : g / 2;
+			grad_data[lo] += wl;
+			if (!(count % 2))
+				grad_data[hi] += wh;
+			if (grad_bg_map) {
+				grad_bg_map[lo] += wl;
+				if (!(count % 2))
+					grad_bg_map[hi] += wh;
+			}
+			if (has_bg)
+				scalar += (wl + wh) - g;
+			break;
+		}
+	}
+	if (grad_bg_scalar)
+		*grad_bg_scalar = scalar;
+	free(pre);
+	free(donor);
+	free(keys);
+	free(idx);
 }

@@ -139,3 +139,34 @@ def laplacian(a, border="mirror"):
     out = np.empty_like(a)
     lib().oracle_laplacian(_ptr(a), _ptr(out), a.shape[1], a.shape[0], BORDERS[border])
     return out
+
+
+def backward(data, crmask, grad, *, mask=None, background=None):
+    """CPU-index reference gradient of a frozen-mask cleaning of one frame.
+
+    Returns (grad_data, grad_background_map or None, grad_background_scalar).
+    """
+    L = lib()
+    if not hasattr(L.oracle_backward, "_set"):
+        L.oracle_backward.argtypes = [ctypes.POINTER(OracleImage), ctypes.POINTER(OracleOptions),
+                                      _bp, _dp, _dp, _dp, _dp]
+        L.oracle_backward._set = True
+    data = _f64(data)
+    h, w = data.shape
+    bgmap, bgs = None, math.nan
+    if background is not None:
+        if np.ndim(background) == 0:
+            bgs = float(background)
+        else:
+            bgmap = _f64(np.broadcast_to(background, data.shape))
+    msk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    im = OracleImage(_ptr(data), None, None, None, _ptr(bgmap), _ptr(msk, _bp), w, h)
+    opts = OracleOptions(0, 0, 0, math.nan, 0, bgs, 1, 3)
+    crm = np.ascontiguousarray(crmask, dtype=np.uint8)
+    g = _f64(grad)
+    gx = np.empty_like(data)
+    gmap = np.empty_like(data) if bgmap is not None else None
+    gs = ctypes.c_double(0.0)
+    L.oracle_backward(ctypes.byref(im), ctypes.byref(opts), _ptr(crm, _bp), _ptr(g), _ptr(gx),
+                      _ptr(gmap), ctypes.byref(gs))
+    return gx, gmap, gs.value

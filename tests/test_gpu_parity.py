@@ -92,7 +92,7 @@ def test_plain_512_noise_model(cuda, oracle):
     from cusmic_b200 import scenes
     sc = scenes.plain_512()
     f = sc.frames[0]
-    frames = [dict(data=f.data)]
+    frames = [dict(data=f.data, gain=2.0, readnoise=5.0, background=0.0)]
     check_against_oracle(oracle, frames, dict(SETTINGS, gain=2.0, readnoise=5.0, background=0.0))
 
 
