@@ -20,6 +20,7 @@ EXPORTS = (
     "remove_cosmics_device", "remove_cosmics_batch_device", "cusmic_ragged_batch_device",
     "cusmic_plan_create", "cusmic_plan_bind", "cusmic_plan_execute", "cusmic_plan_wait",
     "cusmic_plan_passes", "cusmic_plan_profile", "cusmic_plan_backward", "cusmic_plan_destroy",
+    "remove_cosmics_device_noalloc",
 )
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
                 "replace", "restore", "copy")
@@ -94,6 +95,8 @@ def lib():
     L.cusmic_plan_backward.argtypes = [vp, vp, vp, vp, vp, cp, sz]
     L.cusmic_plan_destroy.restype = None
     L.cusmic_plan_destroy.argtypes = [vp]
+    L.remove_cosmics_device_noalloc.restype = ip
+    L.remove_cosmics_device_noalloc.argtypes = [img, opt, vp, vp, vp, cp, sz]
     _lib = L
     return L
 

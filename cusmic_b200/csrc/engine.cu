@@ -889,3 +889,201 @@ extern "C" int cusmic_plan_backward(cusmic_plan *p, const double *grad_clean, do
 		check(cudaStreamSynchronize(s));
 	}, msg, len);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free single-frame entry point.
+//
+// Some callers cannot allocate device memory at the moment they clean a frame:
+// a pipeline that is being captured into a CUDA graph (cudaMalloc/cudaFree are
+// not stream-ordered and cudaFree synchronises the device), a real-time
+// acquisition loop that forbids allocation after start-up, or a process whose
+// caching allocator has already reserved the device.  For them this entry
+// point keeps all of its scratch (descriptor, per-frame state, loop control,
+// work lists, bit planes and target/candidate/seed lists) in the static
+// device array below.  Every GPU that loads this library holds the array until
+// the process exits.  Calls share it: two calls whose work overlaps on the GPU
+// race, so callers serialise them (one stream, or their own ordering).
+
+namespace cb {
+
+constexpr size_t NOALLOC_MAX_PIXELS = 512 * 512;
+constexpr int NOALLOC_MAX_ROWS = 16384;
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(12) << 20; // 12 MiB
+
+static __device__ __align__(256) unsigned char noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Offsets of the scratch segments for a w x h frame (256-byte aligned).
+struct NoallocLayout {
+	size_t desc, state, ctl, offsets, rows, items, bits, targets, cands, seeds, end;
+	int nitems;
+	long long plane;
+};
+
+static NoallocLayout noalloc_layout(int w, int h, bool error_map)
+{
+	auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+	NoallocLayout L{};
+	const size_t n = (size_t)w * h;
+	const int words = (w + 31) / 32;
+	const int rows_per_item = error_map ? STREAM_ROWS : MTILE;
+	L.nitems = ((w + 31) / 32) * ((h + rows_per_item - 1) / rows_per_item);
+	L.plane = (long long)h * words;
+	size_t o = 0;
+	L.desc = o;
+	o = up(o + sizeof(FrameDesc));
+	L.state = o;
+	o = up(o + sizeof(FrameState));
+	L.ctl = o;
+	o = up(o + sizeof(Control));
+	L.offsets = o;
+	o = up(o + sizeof(long long));
+	L.rows = o;
+	o = up(o + (size_t)h * sizeof(int2));
+	L.items = o;
+	o = up(o + (size_t)L.nitems * sizeof(int4));
+	L.bits = o;
+	o = up(o + (size_t)N_PLANES * L.plane * sizeof(uint32_t));
+	L.targets = o;
+	o = up(o + n * sizeof(uint2));
+	L.cands = o;
+	o = up(o + n * sizeof(uint2));
+	L.seeds = o;
+	o = up(o + n * sizeof(Seed));
+	L.end = o;
+	return L;
+}
+
+// Writes the frame descriptor, its row list and its strip (or tile) list
+// into the scratch, so the call needs no host-side staging buffer.
+__global__ void noalloc_setup_kernel(FrameDesc fd, FrameDesc *desc, long long *offsets, int2 *rows,
+	int4 *items, int nitems, int rows_per_item)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i == 0) {
+		*desc = fd;
+		*offsets = 0;
+	}
+	if (i < fd.h)
+		rows[i] = make_int2(0, i);
+	if (i < nitems) {
+		const int tx = (fd.w + 31) / 32;
+		items[i] = make_int4(0, (i % tx) * 32, (i / tx) * rows_per_item, 0);
+	}
+}
+
+struct NoallocDevice {
+	unsigned char *scratch = nullptr;
+	int sms = 0;
+};
+
+// Once per device, with that device current: the device address of the
+// static array (its host-side name is only a stand-in) and the SM count.
+static NoallocDevice noalloc_device(int dev)
+{
+	static std::mutex mu;
+	static NoallocDevice cache[64];
+	if (dev < 0 || dev >= 64)
+		throw std::runtime_error("device ordinal out of range");
+	std::lock_guard<std::mutex> lock(mu);
+	NoallocDevice &d = cache[dev];
+	if (!d.scratch) {
+		void *ptr = nullptr;
+		check(cudaGetSymbolAddress(&ptr, noalloc_scratch));
+		check(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+		d.scratch = static_cast<unsigned char *>(ptr);
+	}
+	return d;
+}
+
+} // namespace cb
+
+extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmic_options *o,
+	double *clean, uint8_t *mask, void *stream, char *msg, size_t len)
+{
+	return guarded([&] {
+		check_arguments(im, 1, o, nullptr, clean, mask, true);
+		if (im->width * im->height > NOALLOC_MAX_PIXELS || im->height > (size_t)NOALLOC_MAX_ROWS)
+			throw InvalidArgument("frame exceeds the static scratch: at most 262144 pixels "
+				"and 16384 rows");
+		int dev;
+		check(cudaGetDevice(&dev));
+		const NoallocDevice nd = noalloc_device(dev);
+		cudaStream_t s = (cudaStream_t)stream;
+		const int w = (int)im->width, h = (int)im->height;
+		const bool error_map = im->error != nullptr;
+		const NoallocLayout L = noalloc_layout(w, h, error_map);
+		if (L.end > NOALLOC_SCRATCH_BYTES)
+			throw InvalidArgument("frame exceeds the static scratch");
+		unsigned char *base = nd.scratch;
+		FrameDesc *frames = reinterpret_cast<FrameDesc *>(base + L.desc);
+		FrameState *state = reinterpret_cast<FrameState *>(base + L.state);
+		Control *ctl = reinterpret_cast<Control *>(base + L.ctl);
+		long long *offsets = reinterpret_cast<long long *>(base + L.offsets);
+		int2 *rows = reinterpret_cast<int2 *>(base + L.rows);
+		int4 *items = reinterpret_cast<int4 *>(base + L.items);
+		uint2 *targets = reinterpret_cast<uint2 *>(base + L.targets);
+		uint2 *cands = reinterpret_cast<uint2 *>(base + L.cands);
+		Seed *seeds = reinterpret_cast<Seed *>(base + L.seeds);
+
+		FrameDesc fd{};
+		fd.data = im->data;
+		fd.error = im->error;
+		fd.gain_map = im->error ? nullptr : im->gain;
+		fd.rn_map = im->error ? nullptr : im->readnoise;
+		fd.bg_map = im->background;
+		fd.mask = im->mask;
+		fd.clean = clean;
+		fd.mask_out = mask;
+		fd.bits = reinterpret_cast<uint32_t *>(base + L.bits);
+		fd.gain = o->gain;
+		fd.rn = o->readnoise;
+		fd.bg = o->background;
+		fd.w = w;
+		fd.h = h;
+		fd.words = (w + 31) / 32;
+		fd.plane = L.plane;
+		fd.has_bg = im->background != nullptr || !std::isnan(o->background);
+		DetectParams prm{};
+		prm.contrast = o->contrast;
+		prm.cr = o->cr_threshold;
+		prm.nb = o->neighbor_threshold;
+		prm.tmin = std::fmin(o->cr_threshold, o->neighbor_threshold);
+		prm.tloose = prm.tmin * (1 - 1e-12);
+		prm.mode = o->border;
+
+		const int setup_n = h > L.nitems ? h : L.nitems;
+		noalloc_setup_kernel<<<(setup_n + 255) / 256, 256, 0, s>>>(fd, frames, offsets, rows, items,
+			L.nitems, error_map ? STREAM_ROWS : MTILE);
+		init_kernel<<<1, 256, 0, s>>>(state, 1, ctl, o->maxiter);
+		const int row_blocks = (h + 7) / 8 < nd.sms * 8 ? (h + 7) / 8 : nd.sms * 8;
+		if (!o->maxiter) {
+			copy_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
+		} else {
+			prepare_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, targets, ctl);
+			replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_holes, 1);
+			for (int it = 0; it < o->maxiter; ++it) {
+				if (error_map) {
+					const int b = (L.nitems + 7) / 8 < nd.sms * 8 ? (L.nitems + 7) / 8 : nd.sms * 8;
+					sig_stream_kernel<<<b, 256, 0, s>>>(frames, state, items, L.nitems, prm, ctl,
+						cands);
+				} else {
+					const int b = L.nitems < nd.sms * 8 ? L.nitems : nd.sms * 8;
+					sig_model_kernel<<<b, 256, 0, s>>>(frames, state, items, L.nitems, prm, ctl,
+						cands);
+				}
+				candidate_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
+				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl);
+				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, targets, ctl);
+				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
+				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, 0);
+			}
+			restore_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
+		}
+		check(cudaGetLastError());
+		FrameState st;
+		check(cudaMemcpyAsync(&st, state, sizeof(st), cudaMemcpyDeviceToHost, s));
+		check(cudaStreamSynchronize(s));
+		if (st.error || (st.holes && st.allowed && !st.finite))
+			throw InvalidArgument("no finite replacement donors");
+	}, msg, len);
+}

@@ -107,6 +107,23 @@ cusmic_plan_backward(cusmic_plan *plan, const double *grad_clean, double *grad_d
 void
 cusmic_plan_destroy(cusmic_plan *plan);
 
+/* remove_cosmics_device for callers that cannot allocate device memory when
+ * they clean a frame: code being captured into a CUDA graph (cudaMalloc and
+ * cudaFree are not stream-ordered; cudaFree synchronises the device), real-time
+ * loops that forbid allocation after start-up, or processes whose allocator
+ * has already reserved the GPU.  Same arguments and results as
+ * remove_cosmics_device, for one frame of at most 262144 pixels and 16384 rows
+ * (larger frames are rejected with CUSMIC_INVALID).  All scratch lives in a
+ * 12 MiB static device array that every GPU loading this library holds until
+ * the process exits; the call allocates nothing.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  Calls share the array: calls whose
+ * work overlaps on the GPU race, so serialise them.  Synchronises before
+ * returning.  No counterpart in the reference. */
+int
+remove_cosmics_device_noalloc(const struct cusmic_image *image, const struct cusmic_options *options,
+	double *clean, uint8_t *mask, void *stream, char *msg, size_t message_size);
+
 #ifdef __cplusplus
 }
 #endif
