@@ -245,7 +245,7 @@ def main():
                 "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4),
                 "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
                 "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
-    launches_per_step = 4 + 6 * max(passes)  # init, prepare, fill, restore + 6 per pass
+    launches_per_step = 4 + 7 * max(passes)  # init, prepare, fill, restore + 7 per pass
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),

@@ -23,7 +23,7 @@ EXPORTS = (
     "remove_cosmics_device_noalloc",
 )
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
-                "replace", "restore", "copy")
+                "replace", "restore", "copy", "low")
 
 
 class Image(ctypes.Structure):

@@ -89,15 +89,19 @@ struct FrameState {
 	unsigned int replace; // this pass flagged new pixels: re-replace targets
 	unsigned int error;   // a target had no finite donor
 	unsigned int passes;  // detection passes run
-	unsigned long long todo, donors;          // this pass: new pixels, donors left
-	unsigned long long holes, allowed, finite; // from preparation
+	// Nonzero-only facts (set to 1 by many warps, never counted):
+	unsigned long long todo, donors;          // this pass: any new pixel, any donor left
+	unsigned long long holes, allowed, finite; // any hole, any allowed pixel, any finite donor
 };
 
 // Loop control shared by the per-pass kernels.
 struct Control {
 	unsigned long long n_targets; // length of the target list
 	unsigned long long n_holes;   // length of the hole list (front of the same buffer)
-	unsigned long long n_cand;    // this pass: pixels whose sig_raw can pass a threshold
+	unsigned long long n_cand;    // this pass: pixels whose sig_raw can exceed cr_threshold
+	unsigned long long n_low;     // this pass: pixels whose sig_raw can only exceed neighbor
+	unsigned long long cand_cap;  // capacity of the candidate buffer (high from the front,
+	                              // low from the back)
 	int iter;                     // detection passes issued so far
 	int maxiter;
 	int any_active;

@@ -49,10 +49,20 @@ namespace cb {
 
 struct DetectParams {
 	double contrast, cr, nb;
-	double tmin;   // min(cr, nb): sig_raw above it can pass a threshold
-	double tloose; // tmin (1 - 1e-12): division-free superset test of kernel A
+	double tmin;  // min(cr, nb): sig_raw above it can pass a threshold
+	double thi2;  // 2 cr (1 - 1e-12): division-free superset test for sig_raw > cr
+	double tlo2;  // 2 nb (1 - 1e-12): the same for sig_raw > neighbor
 	int mode;
 };
+
+// Kernel A's two superset tests (see sig_stream_kernel): bit 0 = can exceed
+// cr_threshold, bit 1 = can only exceed neighbor_threshold.
+__device__ __forceinline__ uint32_t candidate_class(double lap, double nz, const DetectParams &p)
+{
+	if (lap > p.thi2 * nz)
+		return 1u;
+	return lap > p.tlo2 * nz ? 2u : 0u;
+}
 
 // Seed slot of candidate e (frame NO_SEED when the candidate is not a seed).
 struct Seed {
@@ -86,6 +96,17 @@ __device__ __forceinline__ int lap_mode(int mode)
 	return mode == MIRROR || mode == REFLECT ? NEAREST : mode;
 }
 
+// The same Laplacian from quarter values q = x / 4 (exact: a power-of-two
+// scaling), so a streaming kernel can scale each pixel once.
+__device__ __forceinline__ double lap_quarters(double qc, double qu, double qd, double ql, double qr)
+{
+	double up = qc - qu;
+	double down = qc - qd;
+	double left = qc - ql;
+	double right = qc - qr;
+	return (positive(up + left) + positive(up + right)) + (positive(down + left) + positive(down + right));
+}
+
 // clean at (x, y) under a border mode (0 outside for constant).
 __device__ __forceinline__ double clean_at(const FrameDesc &fd, int x, int y, int mode)
 {
@@ -109,43 +130,114 @@ __device__ __forceinline__ void clear_detect_words(const FrameDesc &fd, long lon
 		plane_ptr(fd, P_S1 + lane)[word] = 0u;
 }
 
-// A, error-map frames: one warp per item {frame, x0, y0}: 32 columns from x0,
-// rows y0 .. y0 + STREAM_ROWS - 1, in sub-blocks of STREAM_SUB rows whose
-// loads are all issued before any is used (enough bytes in flight per SM to
-// approach HBM bandwidth).  The rows above and below stay in registers and
-// the left and right neighbours come from adjacent lanes.
-//
-// This kernel only has to find a superset of {sig_raw > tmin}: B evaluates
-// sig_raw exactly for every candidate and drops the others.  So instead of
-// dividing it tests lap > thr * (2 noise) with thr = tmin (1 - 1e-12) (prm.
-// tloose): the product is rounded by at most 2^-53 relative, so every pixel
-// with fl(lap / (2 noise)) > tmin passes (and NaN, infinite or zero noise
-// give the same outcome as the division).
-constexpr int STREAM_SUB = 8;
-
 // Append the candidates of one strip item (lane = column, bit k of `rows` =
-// row y0 + k) with a single atomic per item.
-__device__ __forceinline__ void stream_flush(int f, int w, int x, int y0, uint32_t rows,
+// row y0 + k) with a single atomic per item; the high list grows from the
+// front of the buffer, the low list from its back.
+__device__ __forceinline__ void stream_flush(int f, int w, int x, int y0, uint32_t hi, uint32_t lo,
 	Control *ctl, uint2 *cands)
 {
-	if (!__any_sync(0xffffffffu, rows != 0))
-		return;
-	unsigned long long slot = warp_append(&ctl->n_cand, __popc(rows));
-	while (rows) {
-		const int k = __ffs(rows) - 1;
-		rows &= rows - 1;
-		cands[slot++] = make_uint2((unsigned)f, (unsigned)((long long)(y0 + k) * w + x));
+	if (__any_sync(0xffffffffu, hi != 0)) {
+		unsigned long long slot = warp_append(&ctl->n_cand, __popc(hi));
+		while (hi) {
+			const int k = __ffs(hi) - 1;
+			hi &= hi - 1;
+			cands[slot++] = make_uint2((unsigned)f, (unsigned)((long long)(y0 + k) * w + x));
+		}
+	}
+	if (__any_sync(0xffffffffu, lo != 0)) {
+		unsigned long long slot = warp_append(&ctl->n_low, __popc(lo));
+		while (lo) {
+			const int k = __ffs(lo) - 1;
+			lo &= lo - 1;
+			cands[ctl->cand_cap - 1 - slot++] =
+				make_uint2((unsigned)f, (unsigned)((long long)(y0 + k) * w + x));
+		}
 	}
 }
 
-__global__ void __launch_bounds__(256, 2)
+// A, error-map frames: one warp per item {frame, x0, y0}: 32 columns from x0,
+// rows y0 .. y0 + STREAM_ROWS - 1.  Each warp streams its rows through a
+// shared-memory ring filled with cp.async, SR_LEAD rows ahead of the row it
+// evaluates, so many row loads are in flight per warp without holding
+// registers.  A ring row holds the row's 32 columns plus one halo column on
+// each side, each cell already border-mapped with the Laplacian's border mode
+// (zero outside for constant), so the evaluation has no border cases.
+//
+// The kernel only has to find supersets of {sig_raw > cr} and {sig_raw >
+// neighbor}: B evaluates sig_raw exactly for every candidate and drops the
+// others.  So instead of dividing it tests lap > (2 t (1 - 1e-12)) noise: the
+// product is rounded by at most 2^-53 relative and 2 t scales exactly, so
+// every pixel with fl(lap / (2 noise)) > t passes (NaN, infinite or zero noise
+// give the same outcome as the division, or a larger superset).
+constexpr int SR_DEPTH = 8; // ring rows per warp (power of two)
+constexpr int SR_LEAD = 5;  // rows issued ahead of the row being evaluated
+
+struct StreamRing {
+	double c[SR_DEPTH][34]; // clean, columns x0 - 1 .. x0 + 32
+	double e[SR_DEPTH][32]; // error map, columns x0 .. x0 + 31
+	uint32_t hole[SR_DEPTH];
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+	unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+	unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+	asm volatile("cp.async.commit_group;\n" ::);
+}
+
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+	asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Every lane issues its cells of ring row r (one commit group per row, empty
+// past the last needed row so group counting stays uniform).
+__device__ __forceinline__ void stream_issue(StreamRing &R, const FrameDesc &fd, int r, int r_end,
+	int y0, int y1, int x0, int lane, int lm, int mx, int mx_halo, int xc)
+{
+	if (r <= r_end) {
+		const int slot = r & (SR_DEPTH - 1);
+		const int my = border_index(r, fd.h, lm);
+		const double *row = fd.clean + (long long)(my < 0 ? 0 : my) * fd.w;
+		if (my >= 0 && mx >= 0)
+			cp_async8(&R.c[slot][1 + lane], row + mx);
+		else
+			R.c[slot][1 + lane] = 0.0;
+		if (lane == 0 || lane == 31) {
+			const int hi = lane == 0 ? 0 : 33;
+			if (my >= 0 && mx_halo >= 0)
+				cp_async8(&R.c[slot][hi], row + mx_halo);
+			else
+				R.c[slot][hi] = 0.0;
+		}
+		if (r >= y0 && r < y1) {
+			cp_async8(&R.e[slot][lane], fd.error + (long long)r * fd.w + xc);
+			if (lane == 0)
+				cp_async4(&R.hole[slot], plane_ptr(fd, P_HOLE) + (long long)r * fd.words + (x0 >> 5));
+		}
+	}
+	cp_async_commit();
+}
+
+__global__ void __launch_bounds__(256)
 sig_stream_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const int4 *__restrict__ items, int nitems, DetectParams prm, Control *ctl, uint2 *cands)
 {
+	__shared__ StreamRing rings[8];
 	const int lane = threadIdx.x & 31;
+	StreamRing &R = rings[threadIdx.x >> 5];
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
 	const int lm = lap_mode(prm.mode);
-	const double thr = prm.tloose;
 	for (int it = gw; it < nitems; it += nw) {
 		const int4 item = items[it];
 		if (!state[item.x].active)
@@ -155,68 +247,60 @@ sig_stream_kernel(const FrameDesc *__restrict__ frames, const FrameState *__rest
 		const int x0 = item.y, y0 = item.z, y1 = min(y0 + STREAM_ROWS, h);
 		const int x = x0 + lane, xc = min(x, w - 1);
 		const bool valid = x < w;
-		// Strips away from the left/right frame edges take their halo column
-		// with a plain load (lane 0: x0 - 1, lane 31: x0 + 32).
-		const bool inner = x0 >= 1 && x0 + 32 < w;
-		const int hx = lane == 0 ? x0 - 1 : x0 + 32;
-		const double *__restrict__ clean = fd.clean, *__restrict__ err = fd.error;
-		const uint32_t *holes = plane_ptr(fd, P_HOLE) + (x0 >> 5);
-		double up = clean_at(fd, xc, y0 - 1, lm);
-		double cur = clean[(long long)y0 * w + xc];
-		uint32_t found = 0; // bit k: row y0 + k is a candidate in this lane's column
-		int ys = y0;
-		if (inner) {
-			// Full sub-blocks with a next row inside the frame: no border logic.
-			for (; ys + STREAM_SUB <= y1 && ys + STREAM_SUB < h; ys += STREAM_SUB) {
-				double nxt[STREAM_SUB], nz[STREAM_SUB], halo[STREAM_SUB];
-				uint32_t hw[STREAM_SUB];
-				const double *crow = clean + (long long)ys * w;
-				const double *erow = err + (long long)ys * w;
-#pragma unroll
-				for (int k = 0; k < STREAM_SUB; ++k) {
-					nxt[k] = crow[(long long)(k + 1) * w + xc];
-					nz[k] = erow[(long long)k * w + xc];
-					hw[k] = holes[(long long)(ys + k) * words];
-					halo[k] = (lane == 0 || lane == 31) ? crow[(long long)k * w + hx] : 0.0;
-				}
-#pragma unroll
-				for (int k = 0; k < STREAM_SUB; ++k) {
-					double left = __shfl_up_sync(0xffffffffu, cur, 1);
-					double right = __shfl_down_sync(0xffffffffu, cur, 1);
-					if (lane == 0)
-						left = halo[k];
-					if (lane == 31)
-						right = halo[k];
-					const double lap = lap_formula(cur, up, nxt[k], left, right);
-					const bool c = valid && !((hw[k] >> lane) & 1u) && lap > thr * (2 * nz[k]);
-					found |= (uint32_t)c << (ys + k - y0);
-					clear_detect_words(fd, (long long)(ys + k) * words + (x0 >> 5), lane);
-					up = cur;
-					cur = nxt[k];
-				}
+		const int mx = border_index(x, w, lm);
+		const int mx_halo = border_index(lane == 0 ? x0 - 1 : x0 + 32, w, lm);
+		const int r_end = y1; // the row below the last output row
+		for (int r = y0 - 1; r < y0 - 1 + SR_LEAD + 1; ++r)
+			stream_issue(R, fd, r, r_end, y0, y1, x0, lane, lm, mx, mx_halo, xc);
+		uint32_t hi = 0, lo = 0; // bit k: row y0 + k of this lane's column is a candidate
+		double qu = 0, qc = 0;   // quarter values of the rows above and at y
+		for (int y = y0; y < y1; ++y) {
+			// Groups issued: rows y0 - 1 .. y + SR_LEAD - 1; row y + 1 is done
+			// once at most SR_LEAD - 2 newer groups are pending.
+			cp_async_wait<SR_LEAD - 2>();
+			__syncwarp();
+			const int s = y & (SR_DEPTH - 1), sd = (y + 1) & (SR_DEPTH - 1);
+			if (y == y0) {
+				qu = R.c[(y - 1) & (SR_DEPTH - 1)][1 + lane] * 0.25;
+				qc = R.c[s][1 + lane] * 0.25;
 			}
-		}
-		// Remaining rows, frame edges: one row at a time with border handling.
-#pragma unroll 1
-		for (int y = ys; y < y1; ++y) {
-			const long long row = (long long)y * w;
-			const double down = y + 1 < h ? clean[row + w + xc] : clean_at(fd, xc, y + 1, lm);
-			const double nz = err[row + xc];
-			const uint32_t hw = holes[(long long)y * words];
-			double left = __shfl_up_sync(0xffffffffu, cur, 1);
-			double right = __shfl_down_sync(0xffffffffu, cur, 1);
-			if (lane == 0)
-				left = clean_at(fd, x - 1, y, lm);
-			if (lane == 31 || x + 1 >= w)
-				right = clean_at(fd, x + 1, y, lm);
-			const double lap = lap_formula(cur, up, down, left, right);
-			const bool c = valid && !((hw >> lane) & 1u) && lap > thr * (2 * nz);
-			found |= (uint32_t)c << (y - y0);
+			const double qd = R.c[sd][1 + lane] * 0.25;
+			const double lap = lap_quarters(qc, qu, qd, R.c[s][lane] * 0.25, R.c[s][lane + 2] * 0.25);
+			const uint32_t cls = valid && !((R.hole[s] >> lane) & 1u)
+				? candidate_class(lap, R.e[s][lane], prm) : 0u;
+			hi |= (cls & 1u) << (y - y0);
+			lo |= (cls >> 1) << (y - y0);
+			qu = qc;
+			qc = qd;
 			clear_detect_words(fd, (long long)y * words + (x0 >> 5), lane);
-			up = cur;
-			cur = down;
+			__syncwarp();
+			stream_issue(R, fd, y + SR_LEAD, r_end, y0, y1, x0, lane, lm, mx, mx_halo, xc);
 		}
-		stream_flush(item.x, w, x, y0, found, ctl, cands);
+		cp_async_wait<0>();
+		__syncwarp();
+		stream_flush(item.x, w, x, y0, hi, lo, ctl, cands);
+	}
+}
+
+__device__ __forceinline__ void tile_flush(int f, int w, int x, int ybase, uint32_t hi, uint32_t lo,
+	Control *ctl, uint2 *cands)
+{
+	if (__any_sync(0xffffffffu, hi != 0)) {
+		unsigned long long slot = warp_append(&ctl->n_cand, __popc(hi));
+		while (hi) {
+			const int j = __ffs(hi) - 1;
+			hi &= hi - 1;
+			cands[slot++] = make_uint2((unsigned)f, (unsigned)((long long)(ybase + 8 * j) * w + x));
+		}
+	}
+	if (__any_sync(0xffffffffu, lo != 0)) {
+		unsigned long long slot = warp_append(&ctl->n_low, __popc(lo));
+		while (lo) {
+			const int j = __ffs(lo) - 1;
+			lo &= lo - 1;
+			cands[ctl->cand_cap - 1 - slot++] =
+				make_uint2((unsigned)f, (unsigned)((long long)(ybase + 8 * j) * w + x));
+		}
 	}
 }
 
@@ -226,8 +310,8 @@ sig_stream_kernel(const FrameDesc *__restrict__ frames, const FrameState *__rest
 // rn^2 + ., sqrt and / g are each monotone for g > 0), and the median of a
 // window is at least the minimum m_lo of the tile and its halo, so
 // noise(m_lo) <= noise(med5) and lap / (2 noise(m_lo)) >= sig_raw.  The tile
-// therefore tests lap > thr * (2 noise(m_lo)) with thr = tmin (1 - 1e-12): a
-// superset of {sig_raw > tmin} without any median.  Scalar gain and read
+// therefore applies the superset tests of sig_stream_kernel with noise(m_lo)
+// in place of the noise, without any median.  Scalar gain and read
 // noise make noise(m_lo) one value per tile; maps evaluate it per pixel.
 __global__ void __launch_bounds__(256)
 sig_model_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
@@ -237,24 +321,23 @@ sig_model_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restr
 	__shared__ double wmin[8];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const int mode = prm.mode, lm = lap_mode(mode);
-	const double thr = prm.tloose;
 	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
 		const int4 tile = tiles[t];
 		if (!state[tile.x].active)
 			continue; // block-uniform
 		const FrameDesc &fd = frames[tile.x];
 		const int w = fd.w, h = fd.h, words = fd.words, x0 = tile.y, y0 = tile.z;
-		double lo = INFINITY;
+		double vmin = INFINITY;
 		for (int k = tid; k < MHALO * MHALO; k += 256) {
 			const double v = clean_at(fd, x0 - 2 + k % MHALO, y0 - 2 + k / MHALO, mode);
 			C[k] = v;
-			lo = dmin(lo, v);
+			vmin = dmin(vmin, v);
 		}
 #pragma unroll
 		for (int o = 16; o; o >>= 1)
-			lo = dmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+			vmin = dmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
 		if (lane == 0)
-			wmin[warp] = lo;
+			wmin[warp] = vmin;
 		__syncthreads();
 		double m_lo = wmin[0];
 #pragma unroll
@@ -263,13 +346,13 @@ sig_model_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restr
 		const bool scalar_noise = !fd.gain_map && !fd.rn_map;
 		const double nz_tile = scalar_noise ? noise_from_median(fd, 0, m_lo) : 0.0;
 		const uint32_t *holes = plane_ptr(fd, P_HOLE);
-		uint32_t found = 0; // bit j: row warp + 8 j of this lane's column
+		uint32_t hi = 0, lo = 0; // bit j: row warp + 8 j of this lane's column
 #pragma unroll 1
 		for (int oy = warp; oy < MTILE; oy += 8) {
 			const int x = x0 + lane, y = y0 + oy;
 			if (y >= h)
 				break; // warp-uniform
-			bool c = false;
+			uint32_t cls = 0;
 			if (x < w) {
 				const int cx = lane + 2, cy = oy + 2;
 				double l, r, u, d;
@@ -288,20 +371,15 @@ sig_model_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restr
 				const double nz = scalar_noise ? nz_tile
 					: noise_from_median(fd, (long long)y * w + x, m_lo);
 				const uint32_t hw = holes[(long long)y * words + (x0 >> 5)];
-				c = !((hw >> lane) & 1u) && lap > thr * (2 * nz);
+				cls = (hw >> lane) & 1u ? 0u : candidate_class(lap, nz, prm);
 			}
-			found |= (uint32_t)c << (oy >> 3);
+			hi |= (cls & 1u) << (oy >> 3);
+			lo |= (cls >> 1) << (oy >> 3);
 			clear_detect_words(fd, (long long)y * words + (x0 >> 5), lane);
 		}
-		if (__any_sync(0xffffffffu, found != 0)) {
-			unsigned long long slot = warp_append(&ctl->n_cand, __popc(found));
-			while (found) {
-				const int j = __ffs(found) - 1;
-				found &= found - 1;
-				cands[slot++] = make_uint2((unsigned)tile.x,
-					(unsigned)((long long)(y0 + warp + 8 * j) * w + x0 + lane));
-			}
-		}
+		// Bits j of this lane are rows y0 + warp + 8 j: append as rows of a
+		// strip starting at y0 + warp with stride 8.
+		tile_flush(tile.x, w, x0 + lane, y0 + warp, hi, lo, ctl, cands);
 		__syncthreads();
 	}
 }
@@ -340,6 +418,12 @@ __device__ __forceinline__ double warp_sort32(double v)
 // a 32-lane bitonic network (+inf padding) gives the 5 x 5 median, and
 // sig = sig_raw(center) - median decides the S1/S2 bits and the seed list.  A
 // window holding a NaN takes the reference's exact rule in lane 0.
+//
+// LOW: the low list (sig_raw can exceed only neighbor_threshold), run after
+// the seed kernel.  Only the S2 bit can be set there, and S2 is read only by
+// the second growth step, i.e. within distance 2 of a CAND pixel; candidates
+// with no CAND bit in their clipped 5 x 5 neighbourhood are skipped.
+template <bool LOW>
 __global__ void __launch_bounds__(256)
 candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, Seed *seeds)
@@ -347,13 +431,23 @@ candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__
 	const int lane = threadIdx.x & 31;
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-	const long long n = (long long)ctl->n_cand;
+	const long long n = (long long)(LOW ? ctl->n_low : ctl->n_cand);
 	const int mode = prm.mode, lm = lap_mode(mode);
 	for (long long e = gw; e < n; e += nw) {
-		const uint2 t = cands[e];
+		const uint2 t = cands[LOW ? ctl->cand_cap - 1 - e : e];
 		const FrameDesc &fd = frames[t.x];
 		const int w = fd.w, h = fd.h;
 		const int x = (int)(t.y % (unsigned)w), y = (int)(t.y / (unsigned)w);
+		if (LOW) {
+			bool near = false;
+			if (lane < 25) {
+				const int cx = x + lane % 5 - 2, cy = y + lane / 5 - 2;
+				near = cx >= 0 && cx < w && cy >= 0 && cy < h &&
+					test_bit(plane_ptr(fd, P_CAND), fd.words, cx, cy);
+			}
+			if (!__any_sync(0xffffffffu, near))
+				continue; // warp-uniform
+		}
 		double v = INFINITY, nz = 0;
 		if (lane < 25) {
 			const int mx = border_index(x + lane % 5 - 2, w, mode);
@@ -382,18 +476,18 @@ candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__
 			med = __shfl_sync(0xffffffffu, warp_sort32(v), 12);
 		}
 		const double sig = center - med;
-		bool seed = false;
 		if (lane == 0) {
 			const long long word = (long long)y * fd.words + (x >> 5);
 			const uint32_t bit = 1u << (x & 31);
-			if (sig > prm.cr)
-				atomicOr(plane_ptr(fd, P_S1) + word, bit);
 			if (sig > prm.nb)
 				atomicOr(plane_ptr(fd, P_S2) + word, bit);
-			seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
+			if (!LOW) {
+				if (sig > prm.cr)
+					atomicOr(plane_ptr(fd, P_S1) + word, bit);
+				const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
+				seeds[e] = seed ? Seed{t.x, t.y, sig, nz_center} : Seed{NO_SEED, 0, 0.0, 0.0};
+			}
 		}
-		if (lane == 0)
-			seeds[e] = seed ? Seed{t.x, t.y, sig, nz_center} : Seed{NO_SEED, 0, 0.0, 0.0};
 	}
 }
 

@@ -242,7 +242,8 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 	L.prm.cr = o.cr_threshold;
 	L.prm.nb = o.neighbor_threshold;
 	L.prm.tmin = std::fmin(o.cr_threshold, o.neighbor_threshold);
-	L.prm.tloose = L.prm.tmin * (1 - 1e-12);
+	L.prm.thi2 = 2 * o.cr_threshold * (1 - 1e-12);
+	L.prm.tlo2 = 2 * o.neighbor_threshold * (1 - 1e-12);
 	L.prm.mode = o.border;
 	L.frames.resize(nf);
 	L.bit_off.resize(nf);
@@ -347,7 +348,7 @@ struct GraphLoop {
 
 // Kernel kinds reported by cusmic_plan_profile().
 enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_SIGRAW, K_CAND, K_SEED, K_GROW, K_CONTROL,
-	K_REPLACE, K_RESTORE, K_COPY, K_KINDS };
+	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_KINDS };
 
 // Optional CUDA-event timer: an event after every launch on the launching
 // stream, so each kernel's duration is the gap to the previous event.
@@ -397,11 +398,14 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 			ws.tiles.p, ntiles, L.prm, ws.ctl.p, ws.cands.p);
 	}
 	mark(rec, K_SIGRAW);
-	candidate_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
+	candidate_kernel<false><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
 		ws.seeds.p);
 	mark(rec, K_CAND);
 	seed_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p);
 	mark(rec, K_SEED);
+	candidate_kernel<true><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
+		ws.seeds.p);
+	mark(rec, K_LOW);
 	grow_update_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.rows.p, nrows, ws.targets.p, ws.ctl.p);
 	mark(rec, K_GROW);
@@ -416,7 +420,8 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	Recorder *rec = nullptr)
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
-	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter);
+	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
+		(unsigned long long)L.total_px);
 	mark(rec, K_INIT);
 	if (!L.maxiter) {
 		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
@@ -1048,13 +1053,15 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 		prm.cr = o->cr_threshold;
 		prm.nb = o->neighbor_threshold;
 		prm.tmin = std::fmin(o->cr_threshold, o->neighbor_threshold);
-		prm.tloose = prm.tmin * (1 - 1e-12);
+		prm.thi2 = 2 * o->cr_threshold * (1 - 1e-12);
+		prm.tlo2 = 2 * o->neighbor_threshold * (1 - 1e-12);
 		prm.mode = o->border;
 
 		const int setup_n = h > L.nitems ? h : L.nitems;
 		noalloc_setup_kernel<<<(setup_n + 255) / 256, 256, 0, s>>>(fd, frames, offsets, rows, items,
 			L.nitems, error_map ? STREAM_ROWS : MTILE);
-		init_kernel<<<1, 256, 0, s>>>(state, 1, ctl, o->maxiter);
+		init_kernel<<<1, 256, 0, s>>>(state, 1, ctl, o->maxiter,
+			(unsigned long long)im->width * im->height);
 		const int row_blocks = (h + 7) / 8 < nd.sms * 8 ? (h + 7) / 8 : nd.sms * 8;
 		if (!o->maxiter) {
 			copy_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
@@ -1071,8 +1078,9 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 					sig_model_kernel<<<b, 256, 0, s>>>(frames, state, items, L.nitems, prm, ctl,
 						cands);
 				}
-				candidate_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
+				candidate_kernel<false><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
 				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl);
+				candidate_kernel<true><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
 				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, targets, ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
 				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, 0);

@@ -26,6 +26,23 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 	return v;
 }
 
+__device__ __forceinline__ int warp_inclusive_count(int cnt)
+{
+	const int lane = threadIdx.x & 31;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		int v = __shfl_up_sync(0xffffffffu, cnt, o);
+		if (lane >= o)
+			cnt += v;
+	}
+	return cnt;
+}
+
+__device__ __forceinline__ int warp_exclusive_count(int cnt)
+{
+	return warp_inclusive_count(cnt) - cnt;
+}
+
 // Append `cnt` entries per lane to a global list; returns this lane's first slot.
 __device__ __forceinline__ unsigned long long warp_append(unsigned long long *counter, int cnt)
 {
@@ -45,7 +62,17 @@ __device__ __forceinline__ unsigned long long warp_append(unsigned long long *co
 	return base + (unsigned long long)(incl - cnt);
 }
 
-__global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter)
+// Per-frame facts that the loop control only tests for zero (any hole, any
+// allowed pixel, any new pixel, any donor left): many warps set the same flag
+// with a plain store instead of contending on an atomic counter.
+__device__ __forceinline__ void set_flag(unsigned long long *flag)
+{
+	if (!*(volatile unsigned long long *)flag)
+		*(volatile unsigned long long *)flag = 1;
+}
+
+__global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
+	unsigned long long cand_cap)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < nf) {
@@ -56,6 +83,7 @@ __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter
 	if (i == 0) {
 		Control c = {};
 		c.maxiter = maxiter;
+		c.cand_cap = cand_cap;
 		c.any_active = maxiter > 0;
 		*ctl = c;
 	}
@@ -68,78 +96,115 @@ __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter
 // in flight per SM to approach the HBM bandwidth.
 constexpr int ROW_UNROLL = 4;
 
+// Rows are taken 8 per block iteration (one per warp) with a block-uniform
+// trip count, so the block can gather its hole pixels and append them to the
+// hole list with a single atomic.
 __global__ void __launch_bounds__(256)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
 	int nrows, uint2 *holes_out, Control *ctl)
 {
-	const int lane = threadIdx.x & 31;
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-	for (int r = gw; r < nrows; r += nw) {
-		const int2 item = rows[r];
-		const FrameDesc &fd = frames[item.x];
-		const int w = fd.w, y = item.y, words = fd.words;
-		const long long rowpix = (long long)y * w, roww = (long long)y * words;
-		int holes = 0, allowed = 0, finite = 0;
-		for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
-			double d[ROW_UNROLL], bg[ROW_UNROLL];
-			bool m[ROW_UNROLL];
+	__shared__ int warp_holes[8];
+	__shared__ unsigned long long block_base;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int rb = blockIdx.x * 8; rb < nrows; rb += gridDim.x * 8) {
+		const int r = rb + warp;
+		int nholes = 0;
+		int2 item = make_int2(0, 0);
+		if (r < nrows) {
+			item = rows[r];
+			const FrameDesc &fd = frames[item.x];
+			const int w = fd.w, y = item.y, words = fd.words;
+			const long long rowpix = (long long)y * w, roww = (long long)y * words;
+			uint32_t any_allowed = 0, any_finite = 0;
+			for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
+				double d[ROW_UNROLL], bg[ROW_UNROLL];
+				bool m[ROW_UNROLL];
 #pragma unroll
-			for (int u = 0; u < ROW_UNROLL; ++u) {
-				const int x = xb + 32 * u + lane;
-				d[u] = 0;
-				bg[u] = fd.bg;
-				m[u] = false;
-				if (x < w) {
-					d[u] = fd.data[rowpix + x];
-					if (fd.mask)
-						m[u] = fd.mask[rowpix + x] != 0;
-					if (fd.bg_map)
-						bg[u] = fd.bg_map[rowpix + x];
+				for (int u = 0; u < ROW_UNROLL; ++u) {
+					const int x = xb + 32 * u + lane;
+					d[u] = 0;
+					bg[u] = fd.bg;
+					m[u] = false;
+					if (x < w) {
+						d[u] = fd.data[rowpix + x];
+						if (fd.mask)
+							m[u] = fd.mask[rowpix + x] != 0;
+						if (fd.bg_map)
+							bg[u] = fd.bg_map[rowpix + x];
+					}
+				}
+#pragma unroll
+				for (int u = 0; u < ROW_UNROLL; ++u) {
+					const int x0 = xb + 32 * u;
+					if (x0 >= w)
+						break; // warp-uniform
+					const int x = x0 + lane;
+					const bool valid = x < w;
+					bool hole = false, ok = false, donor = false;
+					if (valid) {
+						hole = !isfinite(d[u]);
+						ok = !hole && !m[u];
+						double c = hole ? 0 : d[u];
+						if (fd.has_bg)
+							c += 1 * bg[u];
+						fd.clean[rowpix + x] = c;
+						donor = ok && isfinite(c);
+					}
+					const uint32_t hw = __ballot_sync(0xffffffffu, hole);
+					const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
+					const uint32_t dw = __ballot_sync(0xffffffffu, donor);
+					any_allowed |= __ballot_sync(0xffffffffu, ok);
+					any_finite |= dw;
+					if (lane < N_PLANES) {
+						uint32_t v = lane == P_HOLE ? hw : lane == P_EXCL ? ew : lane == P_DONOR ? dw : 0u;
+						plane_ptr(fd, lane)[roww + (x0 >> 5)] = v;
+					}
+					nholes += __popc(hw);
 				}
 			}
-#pragma unroll
-			for (int u = 0; u < ROW_UNROLL; ++u) {
-				const int x0 = xb + 32 * u;
-				if (x0 >= w)
-					break; // warp-uniform
-				const int x = x0 + lane;
-				const bool valid = x < w;
-				bool hole = false, ok = false, donor = false;
-				if (valid) {
-					hole = !isfinite(d[u]);
-					ok = !hole && !m[u];
-					double c = hole ? 0 : d[u];
-					if (fd.has_bg)
-						c += 1 * bg[u];
-					fd.clean[rowpix + x] = c;
-					donor = ok && isfinite(c);
-				}
-				const uint32_t hw = __ballot_sync(0xffffffffu, hole);
-				const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
-				const uint32_t dw = __ballot_sync(0xffffffffu, donor);
-				const uint32_t aw = __ballot_sync(0xffffffffu, ok);
-				if (lane < N_PLANES) {
-					uint32_t v = lane == P_HOLE ? hw : lane == P_EXCL ? ew : lane == P_DONOR ? dw : 0u;
-					plane_ptr(fd, lane)[roww + (x0 >> 5)] = v;
-				}
-				holes += __popc(hw);
-				allowed += __popc(aw);
-				finite += __popc(dw);
-				if (hw) {
-					unsigned long long base = warp_append(&ctl->n_holes, hole ? 1 : 0);
-					if (hole)
-						holes_out[base] = make_uint2((unsigned)item.x, (unsigned)(rowpix + x));
-				}
+			if (lane == 0) {
+				if (nholes)
+					set_flag(&state[item.x].holes);
+				if (any_allowed)
+					set_flag(&state[item.x].allowed);
+				if (any_finite)
+					set_flag(&state[item.x].finite);
 			}
 		}
-		if (lane == 0) {
-			if (holes)
-				atomicAdd(&state[item.x].holes, (unsigned long long)holes);
-			if (allowed)
-				atomicAdd(&state[item.x].allowed, (unsigned long long)allowed);
-			if (finite)
-				atomicAdd(&state[item.x].finite, (unsigned long long)finite);
+		if (lane == 0)
+			warp_holes[warp] = nholes;
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			int total = 0;
+			for (int i = 0; i < 8; ++i) {
+				const int c = warp_holes[i];
+				warp_holes[i] = total;
+				total += c;
+			}
+			block_base = total ? atomicAdd(&ctl->n_holes, (unsigned long long)total) : 0ull;
 		}
+		__syncthreads();
+		if (nholes) {
+			// Re-read this row's hole words and write its entries.
+			const FrameDesc &fd = frames[item.x];
+			const uint32_t *hp = plane_ptr(fd, P_HOLE) + (long long)item.y * fd.words;
+			unsigned long long slot = block_base + warp_holes[warp];
+			for (int k0 = 0; k0 < fd.words; k0 += 32) {
+				const int k = k0 + lane;
+				const uint32_t hw = k < fd.words ? hp[k] : 0u;
+				const unsigned long long at = slot + warp_exclusive_count(__popc(hw));
+				uint32_t bits = hw;
+				int j = 0;
+				while (bits) {
+					const int b = __ffs(bits) - 1;
+					bits &= bits - 1;
+					holes_out[at + j++] = make_uint2((unsigned)item.x,
+						(unsigned)((long long)item.y * fd.w + 32 * k + b));
+				}
+				slot += __shfl_sync(0xffffffffu, warp_inclusive_count(__popc(hw)), 31);
+			}
+		}
+		__syncthreads();
 	}
 }
 
@@ -181,7 +246,7 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 		const uint32_t *cand = plane_ptr(fd, P_CAND), *s1 = plane_ptr(fd, P_S1);
 		const uint32_t *s2 = plane_ptr(fd, P_S2), *donor = plane_ptr(fd, P_DONOR);
 		uint32_t *crm = plane_ptr(fd, P_CRMASK);
-		unsigned long long todo = 0, donors = 0;
+		uint32_t todo = 0, donors = 0; // any new pixel / any donor left in this row
 		for (int k0 = 0; k0 < words; k0 += 32) {
 			const int k = k0 + lane;
 			uint32_t fresh = 0;
@@ -202,8 +267,8 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 				const uint32_t now = old | grown;
 				if (fresh)
 					crm[o] = now;
-				todo += __popc(fresh);
-				donors += __popc(donor[o] & ~now);
+				todo |= fresh;
+				donors |= donor[o] & ~now;
 			}
 			if (__any_sync(0xffffffffu, fresh != 0)) {
 				unsigned long long slot = warp_append(&ctl->n_targets, __popc(fresh));
@@ -215,13 +280,13 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 				}
 			}
 		}
-		todo = warp_sum_u64(todo);
-		donors = warp_sum_u64(donors);
+		todo = __any_sync(0xffffffffu, todo != 0);
+		donors = __any_sync(0xffffffffu, donors != 0);
 		if (lane == 0) {
 			if (todo)
-				atomicAdd(&state[item.x].todo, todo);
+				set_flag(&state[item.x].todo);
 			if (donors)
-				atomicAdd(&state[item.x].donors, donors);
+				set_flag(&state[item.x].donors);
 		}
 	}
 }
@@ -259,6 +324,7 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 		int it = ++ctl->iter;
 		ctl->any_active = any;
 		ctl->n_cand = 0;
+		ctl->n_low = 0;
 		if (use_handle)
 			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
 	}

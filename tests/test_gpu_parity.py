@@ -120,7 +120,8 @@ def test_small_shapes(cuda, oracle, mode, shape):
     check_against_oracle(oracle, [frame], dict(SETTINGS, border=mode, gain=1.0, readnoise=3.0))
 
 
-@pytest.mark.parametrize("thresholds", ((0.0, 0.0, 0.0), (1.0, 5.0, 5.0), (3.0, 2.0, 0.5)))
+@pytest.mark.parametrize("thresholds", ((0.0, 0.0, 0.0), (1.0, 5.0, 5.0), (3.0, 2.0, 0.5),
+                                        (2.0, 3.0, 5.0)))
 def test_thresholds(cuda, oracle, thresholds):
     contrast, cr, nb = thresholds
     data, _ = small_scene(11, 48, 64)
