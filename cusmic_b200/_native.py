@@ -23,7 +23,7 @@ EXPORTS = (
     "remove_cosmics_device_noalloc",
 )
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
-                "replace", "restore", "copy", "low")
+                "replace", "restore", "copy", "low", "classify", "floor")
 
 
 class Image(ctypes.Structure):

@@ -89,6 +89,7 @@ struct FrameState {
 	unsigned int replace; // this pass flagged new pixels: re-replace targets
 	unsigned int error;   // a target had no finite donor
 	unsigned int passes;  // detection passes run
+	unsigned int fault;   // a bounded wait inside a kernel ran out (the frame stopped)
 	// Nonzero-only facts (set to 1 by many warps, never counted):
 	unsigned long long todo, donors;          // this pass: any new pixel, any donor left
 	unsigned long long holes, allowed, finite; // any hole, any allowed pixel, any finite donor
@@ -105,6 +106,8 @@ struct Control {
 	int iter;                     // detection passes issued so far
 	int maxiter;
 	int any_active;
+	int ticket;                   // next item of the bulk detection kernel (reset every pass)
+	int fault;                    // a bounded wait ran out in this pass
 	int pad;
 };
 

@@ -438,6 +438,13 @@ candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__
 		const FrameDesc &fd = frames[t.x];
 		const int w = fd.w, h = fd.h;
 		const int x = (int)(t.y % (unsigned)w), y = (int)(t.y / (unsigned)w);
+		// Holes have sig = 0 (src/filters.cuh:137-146): no bit, no seed.  The
+		// bulk dense kernel does not test the hole plane itself.
+		if (test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y)) {
+			if (!LOW && lane == 0)
+				seeds[e] = Seed{NO_SEED, 0, 0.0, 0.0};
+			continue; // warp-uniform
+		}
 		if (LOW) {
 			bool near = false;
 			if (lane < 25) {

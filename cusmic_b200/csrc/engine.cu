@@ -11,6 +11,7 @@
 #include "../../include/cusmic_b200.h"
 #include "common.cuh"
 #include "detect.cuh"
+#include "bulk.cuh"
 #include "kernels.cuh"
 #include "backward.cuh"
 
@@ -18,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -99,7 +101,11 @@ struct Layout {
 	std::vector<FrameDesc> frames;
 	std::vector<long long> bit_off; // word offset of each frame's planes
 	std::vector<int4> tiles; // sig_model_kernel tiles (noise-model frames)
-	std::vector<int4> strips; // sig_stream_kernel items (error-map frames)
+	std::vector<int4> strips; // sig_stream_kernel items (error-map frames, other layouts)
+	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, floor base} (see bulk_eligible)
+	std::vector<FloorJob> floor_jobs; // 32 x 32 blocks of each distinct error map of bulk frames
+	std::vector<long long> floor_base; // per frame: first floor of its map (-1: none)
+	long long nfloors = 0;
 	std::vector<int2> rows;
 	std::vector<long long> offsets; // first output pixel of each frame
 	long long total_words = 0;
@@ -136,6 +142,11 @@ struct Workspace {
 	DevBuf<uint2> cands;
 	DevBuf<Seed> seeds;
 	DevBuf<int4> strips;
+	DevBuf<int4> bulk;
+	DevBuf<FloorJob> fjobs;
+	DevBuf<double> floors;
+	DevBuf<PreCand> pre;
+	DevBuf<int> pre_counts;
 	DevBuf<Control> ctl;
 	DevBuf<long long> offsets;
 	PinBuf<unsigned char> stage;
@@ -233,6 +244,16 @@ static void check_arguments(const cusmic_image *ims, size_t nf, const cusmic_opt
 	}
 }
 
+// The bulk detection kernel copies whole row segments of clean and of the
+// error map with cp.async.bulk, which needs 16-byte aligned addresses and
+// sizes: both buffers 16-byte aligned and an even width (so every row of both
+// starts on a 16-byte boundary).
+static bool bulk_eligible(const FrameDesc &d)
+{
+	return d.error && d.w % 2 == 0 && ((uintptr_t)d.clean & 15) == 0 &&
+		((uintptr_t)d.error & 15) == 0;
+}
+
 static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
 	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask)
 {
@@ -247,6 +268,8 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 	L.prm.mode = o.border;
 	L.frames.resize(nf);
 	L.bit_off.resize(nf);
+	L.floor_base.assign(nf, -1);
+	std::map<const double *, std::vector<std::pair<int, long long>>> maps; // error map -> {frame, base}
 	size_t px = 0;
 	long long words = 0;
 	for (size_t f = 0; f < nf; ++f) {
@@ -276,7 +299,30 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		px += (size_t)d.w * d.h;
 		for (int y = 0; y < d.h; ++y)
 			L.rows.push_back(make_int2((int)f, y));
-		if (d.error) {
+		if (d.error && bulk_eligible(d)) {
+			// Frames of the same shape that share an error map share its floors.
+			long long base = -1;
+			for (const auto &m : maps[d.error])
+				if (L.frames[m.first].w == d.w && L.frames[m.first].h == d.h)
+					base = m.second;
+			if (base < 0) {
+				base = L.nfloors;
+				maps[d.error].push_back({(int)f, base});
+				const int bw = (d.w + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
+				const int bh = (d.h + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
+				for (int by = 0; by < bh; ++by)
+					for (int bx = 0; bx < bw; ++bx)
+						L.floor_jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK, 0,
+							base + (long long)by * bw + bx});
+				L.nfloors += (long long)bw * bh;
+			}
+			if (base > INT_MAX)
+				throw std::bad_alloc();
+			L.floor_base[f] = base;
+			for (int ty = 0; ty < d.h; ty += BK_ROWS)
+				for (int tx = 0; tx < d.w; tx += BK_COLS)
+					L.bulk.push_back(make_int4((int)f, tx, ty, (int)base));
+		} else if (d.error) {
 			for (int ty = 0; ty < d.h; ty += STREAM_ROWS)
 				for (int tx = 0; tx < d.w; tx += 32)
 					L.strips.push_back(make_int4((int)f, tx, ty, 0));
@@ -306,6 +352,13 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	ws.state.ensure(nf);
 	ws.tiles.ensure(L.tiles.size() ? L.tiles.size() : 1);
 	ws.strips.ensure(L.strips.size() ? L.strips.size() : 1);
+	ws.bulk.ensure(L.bulk.size() ? L.bulk.size() : 1);
+	ws.fjobs.ensure(L.floor_jobs.size() ? L.floor_jobs.size() : 1);
+	ws.floors.ensure(L.nfloors ? (size_t)L.nfloors : 1);
+	if (L.maxiter && !L.bulk.empty()) {
+		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
+		ws.pre_counts.ensure(L.bulk.size() * BK_CWARPS);
+	}
 	ws.rows.ensure(L.rows.size());
 	ws.ctl.ensure(1);
 	ws.offsets.ensure(nf);
@@ -319,7 +372,8 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
 	size_t bytes_f = nf * sizeof(FrameDesc), bytes_t = L.tiles.size() * sizeof(int4);
 	size_t bytes_s = L.strips.size() * sizeof(int4), bytes_r = L.rows.size() * sizeof(int2);
-	ws.stage.ensure(bytes_f + bytes_t + bytes_s + bytes_r);
+	size_t bytes_b = L.bulk.size() * sizeof(int4), bytes_j = L.floor_jobs.size() * sizeof(FloorJob);
+	ws.stage.ensure(bytes_f + bytes_t + bytes_s + bytes_r + bytes_b + bytes_j);
 	// The previous call using this workspace synchronised before returning,
 	// so the staging buffer is free.
 	unsigned char *st = ws.stage.p;
@@ -327,6 +381,8 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	std::memcpy(st + bytes_f, L.tiles.data(), bytes_t);
 	std::memcpy(st + bytes_f + bytes_t, L.strips.data(), bytes_s);
 	std::memcpy(st + bytes_f + bytes_t + bytes_s, L.rows.data(), bytes_r);
+	std::memcpy(st + bytes_f + bytes_t + bytes_s + bytes_r, L.bulk.data(), bytes_b);
+	std::memcpy(st + bytes_f + bytes_t + bytes_s + bytes_r + bytes_b, L.floor_jobs.data(), bytes_j);
 	check(cudaMemcpyAsync(ws.frames.p, st, bytes_f, cudaMemcpyHostToDevice, s));
 	if (bytes_t)
 		check(cudaMemcpyAsync(ws.tiles.p, st + bytes_f, bytes_t, cudaMemcpyHostToDevice, s));
@@ -335,6 +391,12 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 			cudaMemcpyHostToDevice, s));
 	check(cudaMemcpyAsync(ws.rows.p, st + bytes_f + bytes_t + bytes_s, bytes_r,
 		cudaMemcpyHostToDevice, s));
+	if (bytes_b)
+		check(cudaMemcpyAsync(ws.bulk.p, st + bytes_f + bytes_t + bytes_s + bytes_r, bytes_b,
+			cudaMemcpyHostToDevice, s));
+	if (bytes_j)
+		check(cudaMemcpyAsync(ws.fjobs.p, st + bytes_f + bytes_t + bytes_s + bytes_r + bytes_b,
+			bytes_j, cudaMemcpyHostToDevice, s));
 	// Offsets are only read by the adjoint; a synchronous copy is fine.
 	check(cudaStreamSynchronize(s));
 	check(cudaMemcpy(ws.offsets.p, L.offsets.data(), nf * sizeof(long long),
@@ -348,7 +410,7 @@ struct GraphLoop {
 
 // Kernel kinds reported by cusmic_plan_profile().
 enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_SIGRAW, K_CAND, K_SEED, K_GROW, K_CONTROL,
-	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_KINDS };
+	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_CLASSIFY, K_FLOOR, K_KINDS };
 
 // Optional CUDA-event timer: an event after every launch on the launching
 // stream, so each kernel's duration is the gap to the previous event.
@@ -387,6 +449,16 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
 	const int ntiles = (int)L.tiles.size(), nstrips = (int)L.strips.size();
+	const int nbulk = (int)L.bulk.size();
+	if (nbulk) {
+		const int cap = di.sms * BK_BLOCKS_PER_SM;
+		sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.bulk.p, nbulk, ws.floors.p, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
+		mark(rec, K_SIGRAW);
+		classify_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk,
+			ws.pre.p, ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
+		mark(rec, K_CLASSIFY);
+	}
 	if (nstrips) {
 		int blocks = (nstrips + 7) / 8, cap = di.sms * 8;
 		sig_stream_kernel<<<blocks < cap ? blocks : cap, 256, 0, s>>>(ws.frames.p, ws.state.p,
@@ -397,7 +469,8 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 		sig_model_kernel<<<ntiles < cap ? ntiles : cap, 256, 0, s>>>(ws.frames.p, ws.state.p,
 			ws.tiles.p, ntiles, L.prm, ws.ctl.p, ws.cands.p);
 	}
-	mark(rec, K_SIGRAW);
+	if (nstrips || ntiles)
+		mark(rec, K_SIGRAW);
 	candidate_kernel<false><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
 		ws.seeds.p);
 	mark(rec, K_CAND);
@@ -423,6 +496,12 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
 		(unsigned long long)L.total_px);
 	mark(rec, K_INIT);
+	if (L.maxiter && !L.floor_jobs.empty()) {
+		const int nj = (int)L.floor_jobs.size(), cap = di.sms * 8;
+		errfloor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p,
+			ws.fjobs.p, nj, ws.floors.p);
+		mark(rec, K_FLOOR);
+	}
 	if (!L.maxiter) {
 		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
 		mark(rec, K_COPY);
@@ -459,6 +538,17 @@ static void enqueue_plain(Workspace &ws, const Layout &L, const DeviceInfo &di, 
 	check(cudaGetLastError());
 }
 
+// Status of one frame after a call: a kernel whose bounded wait ran out is a
+// CUDA-level failure; a target without finite donors is the reference's
+// "no finite replacement donors" (src/cleaner.cuh:95-96,137-138).
+static void check_state(const FrameState &st)
+{
+	if (st.fault)
+		throw std::runtime_error("a detection kernel gave up waiting for its copies");
+	if (st.error || (st.holes && st.allowed && !st.finite))
+		throw InvalidArgument("no finite replacement donors");
+}
+
 // Copy per-frame state back and turn it into a status (stream must be idle
 // after this returns).
 static void finish(Workspace &ws, size_t nf, cudaStream_t s, std::vector<int> *passes = nullptr)
@@ -473,8 +563,7 @@ static void finish(Workspace &ws, size_t nf, cudaStream_t s, std::vector<int> *p
 		const FrameState &st = ws.hstate.p[f];
 		if (passes)
 			(*passes)[f] = (int)st.passes;
-		if (st.error || (st.holes && st.allowed && !st.finite))
-			throw InvalidArgument("no finite replacement donors");
+		check_state(st);
 	}
 }
 
@@ -758,6 +847,12 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 			check(cudaStreamSynchronize(p->last));
 		Layout L = make_layout(ims, nf, p->options, p->scalars.empty() ? nullptr : p->scalars.data(),
 			clean, mask);
+		// The plan's work lists are fixed: frames must keep their detection
+		// kernel (16-byte alignment of the bulk frames) and their sharing of
+		// error maps.
+		if (L.bulk.size() != p->L.bulk.size() || L.strips.size() != p->L.strips.size() ||
+			L.floor_base != p->L.floor_base)
+			throw InvalidArgument("rebound buffers must keep the plan's alignment and map sharing");
 		for (size_t f = 0; f < nf; ++f)
 			L.frames[f].bits = p->L.frames[f].bits;
 		p->ims.assign(ims, ims + nf);
@@ -797,9 +892,7 @@ extern "C" int cusmic_plan_wait(cusmic_plan *p, char *msg, size_t len)
 		check(cudaStreamSynchronize(p->last));
 		check(cudaGetLastError());
 		for (size_t f = 0; f < p->L.frames.size(); ++f) {
-			const FrameState &st = p->ws.hstate.p[f];
-			if (st.error || (st.holes && st.allowed && !st.finite))
-				throw InvalidArgument("no finite replacement donors");
+			check_state(p->ws.hstate.p[f]);
 		}
 	}, msg, len);
 }
@@ -864,9 +957,7 @@ extern "C" int cusmic_plan_backward(cusmic_plan *p, const double *grad_clean, do
 		check(cudaStreamSynchronize(p->last));
 		const size_t nf = p->L.frames.size();
 		for (size_t f = 0; f < nf; ++f) {
-			const FrameState &st = p->ws.hstate.p[f];
-			if (st.error || (st.holes && st.allowed && !st.finite))
-				throw InvalidArgument("no finite replacement donors");
+			check_state(p->ws.hstate.p[f]);
 		}
 		bool map_mode = false;
 		for (const FrameDesc &d : p->L.frames)
@@ -1091,7 +1182,6 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 		FrameState st;
 		check(cudaMemcpyAsync(&st, state, sizeof(st), cudaMemcpyDeviceToHost, s));
 		check(cudaStreamSynchronize(s));
-		if (st.error || (st.holes && st.allowed && !st.finite))
-			throw InvalidArgument("no finite replacement donors");
+		check_state(st);
 	}, msg, len);
 }

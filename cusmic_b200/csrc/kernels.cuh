@@ -300,12 +300,16 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 	int use_handle)
 {
 	int any = 0;
+	const int fault = ctl->fault;
 	for (int f = threadIdx.x; f < nf; f += blockDim.x) {
 		FrameState s = state[f];
 		s.replace = 0;
 		if (s.active) {
 			++s.passes;
-			if (s.todo && !s.donors) {
+			if (fault) { // this pass's detection is incomplete: stop, report
+				s.fault = 1;
+				s.active = 0;
+			} else if (s.todo && !s.donors) {
 				s.error = 1;
 				s.active = 0;
 			} else if (s.todo) {
@@ -325,6 +329,7 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 		ctl->any_active = any;
 		ctl->n_cand = 0;
 		ctl->n_low = 0;
+		ctl->ticket = 0;
 		if (use_handle)
 			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
 	}

@@ -315,3 +315,31 @@ def test_reference_library_parity(cuda, workload):
     for (c1, m1), (c2, m2) in zip(mine.outputs(), theirs.outputs()):
         np.testing.assert_array_equal(m1, m2)
         assert_bits_equal(c1, c2)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("shape", ((1, 2), (2, 2), (5, 4), (33, 2), (31, 256), (40, 258),
+                                   (70, 94), (65, 512), (37, 514), (3, 1000)))
+def test_error_map_even_widths(cuda, oracle, mode, shape):
+    """Even widths with an error map run the bulk-copy detection kernel (rows
+    16-byte aligned); holes, a mask and a background map exercise every bit."""
+    h, w = shape
+    data, mask = small_scene(h * 1000 + w, h, w, holes=0.01, masked=0.02,
+                             rays=max(1, h * w // 40))
+    rng = np.random.default_rng(w)
+    frame = dict(data=data, mask=mask, background=rng.uniform(0, 50, data.shape),
+                 error=np.sqrt(np.abs(np.nan_to_num(data)) + 9))
+    check_against_oracle(oracle, [frame], dict(SETTINGS, border=mode))
+
+
+@pytest.mark.parametrize("mode", ("mirror", "wrap", "constant"))
+def test_ragged_error_maps_mixed_alignment(cuda, oracle, mode):
+    """A ragged batch whose frames alternate between the bulk kernel (even
+    width, aligned offset) and the strip kernel (odd width, or an offset that
+    an odd-sized frame before it left 8 bytes off a 16-byte boundary)."""
+    frames = []
+    for i, (h, w) in enumerate(((40, 300), (17, 33), (64, 256), (33, 130), (9, 7), (50, 514))):
+        data, mask = small_scene(60 + i, h, w, holes=0.005, masked=0.01, rays=max(2, h * w // 60))
+        frames.append(dict(data=data, mask=mask, error=np.sqrt(np.abs(np.nan_to_num(data)) + 9),
+                           background=float(10 * i)))
+    check_against_oracle(oracle, frames, dict(SETTINGS, border=mode), ragged=True)
