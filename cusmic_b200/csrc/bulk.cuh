@@ -1,56 +1,74 @@
-// Dense detection for error-map frames whose rows can be moved by the bulk
-// copy engine: clean 16-byte aligned and an even width (so every row starts on
-// a 16-byte boundary).
+// Dense detection pass: one streaming kernel for every frame of a batch,
+// whatever its width, alignment or noise model.
 //
 // What the pass needs from every pixel is only whether its sig_raw =
-// lap / (2 error) can exceed min(cr_threshold, neighbor_threshold); the exact
+// lap / (2 noise) can exceed min(cr_threshold, neighbor_threshold); the exact
 // value matters for the ~1% of pixels where it can.  So the work is split:
 //
-//  * errfloor_kernel (once per call): the floor of every 32 x 32 block of each
-//    distinct error map, floor = min(max(error, 0)) (NaN counts as 0);
-//  * sig_bulk_kernel (every pass): the Laplacian of every pixel, compared with
-//    2 min(cr, nb) (1 - 1e-12) x floor of its block.  Since error >= floor,
-//    every pixel whose sig_raw exceeds min(cr, nb) passes (the product is
-//    rounded by at most 2^-53 relative, the margin is 1e-12); the error map
-//    itself is not read.  Passing pixels are written with their Laplacian to
-//    a per-warp region of the `pre` list;
-//  * classify_kernel: sig_raw = lap / (2 error) in the reference's operation
-//    order for each listed pixel; above cr_threshold -> high candidate list,
-//    else above neighbor_threshold -> low list (src/filters.cuh:125-135).
+//  * floor_kernel (once per call, after the hole fill): a lower bound of the
+//    noise over every 32 x 32 block, turned into a threshold T = 2 min(cr, nb)
+//    (1 - 1e-12) x floor.  With an error map the floor is min(max(error, 0))
+//    over the block (NaN counts as 0), once for each distinct map.  With the
+//    noise model (src/filters.cuh:107-123) the kernel stores the smallest
+//    clean value of the block (as an ordered key) and the block's largest gain
+//    and smallest read noise.  Between passes only replacement changes clean,
+//    and replace_kernel lowers the key of the block it writes into, so the key
+//    stays a lower bound of the block's values.  Every 5 x 5 median window of
+//    a block lies in the block's 3 x 3 neighbourhood of blocks (border-mapped
+//    positions included; wrap adds the blocks at the opposite edges, constant
+//    adds zero), so the smallest key there bounds every window's median from
+//    below, and the model evaluated at it with the block's gain and read noise
+//    bounds the noise from below: the model is non-decreasing in the median
+//    and in the read noise and non-increasing in the gain;
+//  * sig_bulk_kernel (every pass): the Laplacian of every pixel against T of
+//    its block.  Every pixel whose sig_raw exceeds min(cr, nb) passes (the
+//    product is rounded by at most 2^-53 relative, the margin is 1e-12 and
+//    the upper bound of the Laplacian used here is never below the
+//    reference's value).  Passing pixels are written with that bound to a
+//    per-warp region of the `pre` list (no atomics);
+//  * classify_kernel: sig_raw of each listed pixel, lap / (2 noise), with the
+//    exact noise (error map, or the noise model from the pixel's own 5 x 5
+//    median); above cr_threshold -> high candidate list, else above
+//    neighbor_threshold -> low list (src/filters.cuh:125-135).  The
+//    candidate kernels recompute every value they threshold exactly, so the
+//    lists only have to be supersets.
 //
-// sig_bulk_kernel is warp-specialised.  One producer warp issues
-// `cp.async.bulk` copies of whole clean row segments (BK_COLS columns plus a
-// 2-column halo on each side) into a ring of BK_SLOTS rows in shared memory,
-// one "full" mbarrier per ring row (transaction bytes); it also clears the
-// S1/S2/CAND bit words of the rows it issues.  Four consumer warps evaluate
-// the rows; each of them arrives on the ring row's "empty" mbarrier when it
-// is done with it, which lets the producer reuse the row.  A block takes
-// items of BK_COLS x BK_ROWS pixels from a ticket counter (items of frames
-// that stopped are skipped there) and the ring runs straight through from one
-// item into the next.
+// sig_bulk_kernel is warp-specialised.  One producer warp copies clean row
+// segments (BK_COLS columns plus halo columns) into a ring of BK_SLOTS rows in
+// shared memory: lane 0 issues one `cp.async.bulk` for the 16-byte aligned
+// body of a row, lane 1 copies up to four single elements with 8-byte
+// `cp.async` (an unaligned first or last element, the border columns -1 and
+// w), so rows of any width and alignment stream the same way.  A row whose
+// aligned body starts on an odd cell is stored one cell to the right (its
+// shift).  Each ring row has a "full" mbarrier (lane 0's transaction bytes
+// plus lane 1's cp.async arrive) and an "empty" mbarrier on which each of the
+// four consumer warps arrives when it is done with the row.  The producer also
+// clears the S1/S2/CAND bit words of the rows it issues.  A block takes items
+// of BK_COLS x BK_ROWS pixels from a ticket counter (items of frames that
+// stopped are skipped there) and the ring runs straight through from one item
+// into the next.
 //
 // The Laplacian (src/filters.cuh:86-105): each consumer thread evaluates two
 // column pairs (x, x + 1) and (x + 256, x + 257) and keeps the quarter values
-// of the rows above and at the current row in registers.  Differences the
-// reference computes twice are computed once: down(y) = q(y) - q(y+1) and
-// up(y+1) = q(y+1) - q(y) are exact negatives of each other in
-// round-to-nearest, and so are right(x) and left(x+1).  Negation changes at
-// most the sign of a zero difference.  positive(v) keeps v when its sign bit
-// is clear and gives +0 otherwise (integer operations): equal to the
-// reference's `v < 0 ? 0 : v` for every non-NaN v up to the sign of a zero.
-// No zero sign reaches a strict comparison with a threshold, so for finite
-// inputs the listed Laplacian is the reference's value; where a term is NaN
-// the reference's sig_raw is NaN and its pixel is never a candidate, and a
-// finite value here only lists a pixel that the candidate kernel drops.
+// of the rows above and at the current row, and the current row's left and
+// right neighbours, in registers.  Differences the reference computes twice
+// are computed once: down(y) = q(y) - q(y+1) and up(y+1) = q(y+1) - q(y) are
+// exact negatives of each other in round-to-nearest, and so are right(x) and
+// left(x+1); negation changes at most the sign of a zero difference.
+// positive(v) is replaced by an upper bound: v with its high word cleared when
+// the sign bit is set (0 or a subnormal instead of the reference's 0 for a
+// negative v).  Floating-point addition is monotone, so the sum is never below
+// the reference's Laplacian for finite inputs; where a term is NaN the
+// reference's sig_raw is NaN and its pixel is never a candidate, and a value
+// here only lists a pixel that the candidate kernel drops.
 //
 // Non-finite input pixels (holes, sig = 0 in the reference) are not tested
 // here; the candidate kernel drops candidates that are holes.
 //
 // Borders (Laplacian border mode: nearest for mirror and reflect): rows
 // outside the frame are copied from their border-mapped row, or from a zero
-// row in constant mode.  Columns -1 and w come from 16-byte copies of columns
-// w-2..w-1 and 0..1 (wrap) or of zeros (constant); in nearest mode the thread
-// at the frame edge uses its own column instead.
+// row in constant mode; columns -1 and w are copied from their border-mapped
+// columns (zeros in constant mode), so the evaluation has no border cases.
 //
 // Every wait is bounded (about one second of SM clock).  A wait that runs out
 // sets Control::fault (the loop-control kernel then stops every active frame
@@ -69,37 +87,40 @@ constexpr int BK_HALF = 64 * BK_CWARPS;          // columns of one pair set (256
 constexpr int BK_COLS = 2 * BK_HALF;             // columns per item (512)
 constexpr int BK_ROWS = 32;                      // rows per item
 constexpr int BK_SLOTS = 8;                      // ring rows (power of two)
-constexpr int BK_CELLS = BK_COLS + 4;            // cells of a ring row: columns x0 - 2 .. x0 + BK_COLS + 1
+constexpr int BK_CELLS = BK_COLS + 4;            // cells of a row: columns x0 - 2 .. x0 + BK_COLS + 1
+constexpr int BK_STRIDE = BK_CELLS + 2;          // ring row length: room for a shift of one cell
 constexpr int BK_BLOCKS_PER_SM = 6;
 constexpr int BK_REGION = 4 * 32 * BK_ROWS;      // pre-list entries one consumer warp can write per item
-constexpr int FLOOR_BLOCK = 32;                  // error-map floor granularity (square)
+constexpr int FLOOR_BLOCK = 32;                  // noise-floor granularity (square)
 constexpr long long BK_WAIT_CYCLES = 1LL << 31;
 static_assert((BK_SLOTS & (BK_SLOTS - 1)) == 0, "ring depth must be a power of two");
 static_assert(BK_ROWS == FLOOR_BLOCK, "an item spans one row of floor blocks");
 static_assert(BK_HALF % FLOOR_BLOCK == 0, "pair sets start on a floor block");
+static_assert((BK_STRIDE * 8) % 16 == 0, "ring rows must stay 16-byte aligned");
 
 struct __align__(128) BulkRing {
-	double c[BK_SLOTS][BK_CELLS]; // clean (4128 B per row: a multiple of 16)
-	int2 meta[BK_SLOTS];          // first ring row of an item: {item index, y1}; index < 0: end
+	double c[BK_SLOTS][BK_STRIDE]; // clean; column x0 - 2 + c at cell c + shift
+	int2 meta[BK_SLOTS];           // first ring row of an item: {item index, y1}; index < 0: end
+	int shift[BK_SLOTS];           // 0 or 1
 	unsigned long long full[BK_SLOTS], empty[BK_SLOTS];
 	int abort;
 };
 
-// A pixel that passed the floor test, with its Laplacian.
+// A pixel that passed the floor test, with its Laplacian bound.
 struct PreCand {
 	unsigned pixel, frame;
 	double lap;
 };
 
-// One 32 x 32 block of a frame's error map whose floor errfloor_kernel
-// computes (frames sharing a map share its floors: one job per block of each
-// distinct map).
+// One 32 x 32 block whose threshold floor_kernel computes: kind FLOOR_ERROR
+// (error map; frames that share a map share its thresholds) or FLOOR_MODEL.
+enum FloorKind { FLOOR_ERROR = 0, FLOOR_MODEL = 1 };
 struct FloorJob {
-	int frame, x0, y0, pad;
-	long long out; // index into the floor array
+	int frame, x0, y0, kind;
+	long long out; // index into the threshold array
 };
 
-// Zeros for constant-mode rows outside the frame and constant-mode halos.
+// Zeros for constant-mode rows and columns outside the frame.
 __device__ __align__(16) double bulk_zero_row[BK_CELLS];
 
 __device__ __forceinline__ unsigned smem_u32(const void *p)
@@ -121,6 +142,12 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned b
 __device__ __forceinline__ void mbar_arrive(unsigned long long *b)
 {
 	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Arrive on b once every cp.async this thread issued so far has landed.
+__device__ __forceinline__ void mbar_arrive_cp_async(unsigned long long *b)
+{
+	asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(b)) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_test(unsigned long long *b, unsigned parity)
@@ -159,87 +186,178 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned b
 		: "memory");
 }
 
-// What ring row r of an item starting at column x0 needs copied: the clean
-// cells [cell, cell + n) from clean + src (elements) and up to two 16-byte
-// halo chunks.
+// The copies of ring row r of an item starting at column x0 of a w x h frame
+// whose clean buffer starts `mis` elements past a 16-byte boundary (0 or 1).
+// Cells are relative to the row's shift.
 struct BulkRow {
-	long long src;  // element offset into clean of the main copy (-1: zero row)
-	int cell, n;    // destination cell and element count of the main copy
-	long long lsrc; // halo chunk at cells 0..1: -1 none, -2 zeros, else clean offset
-	long long rsrc; // halo chunk at cells rcell..rcell+1: -1 none, -2 zeros, else clean offset
-	int rcell;
-	unsigned bytes; // transaction bytes of the row
+	int shift;         // 0 or 1
+	long long src;     // body: element offset into clean (-1: the zero row)
+	int cell, n;       // body: destination cell and element count (even, maybe 0)
+	// Single-element copies: an unaligned first element (head), an odd last
+	// element (tail), columns -1 (left) and w (right).  Source: element
+	// offset into clean, -1 for a zero, NO_COPY when there is none.
+	long long hsrc, tsrc, lsrc, rsrc;
+	int hcell, tcell, lcell, rcell;
+	unsigned bytes; // transaction bytes of the body
 };
+constexpr long long NO_COPY = -2;
 
-CB_HD BulkRow bulk_row(int w, int h, int lm, int x0, int r)
+CB_HD BulkRow bulk_row(int w, int h, int lm, int mis, int x0, int r)
 {
 	BulkRow b;
+	b.hsrc = b.tsrc = b.lsrc = b.rsrc = NO_COPY;
+	b.hcell = b.tcell = b.lcell = b.rcell = 0;
 	const int my = border_index(r, h, lm);
-	b.lsrc = b.rsrc = -1;
-	b.rcell = 0;
 	if (my < 0) { // constant mode, row outside the frame
+		b.shift = 0;
 		b.src = -1;
 		b.cell = 0;
 		b.n = BK_CELLS;
-	} else {
-		const int a = x0 - 2 < 0 ? 0 : x0 - 2;
-		const int e = x0 + BK_COLS + 2 < w ? x0 + BK_COLS + 2 : w;
-		b.src = (long long)my * w + a;
-		b.cell = a - (x0 - 2);
-		b.n = e - a;
-		if (lm != NEAREST) {
-			if (x0 == 0)
-				b.lsrc = lm == WRAP ? (long long)my * w + w - 2 : -2;
-			if (w <= x0 + BK_COLS) {
-				b.rsrc = lm == WRAP ? (long long)my * w : -2;
-				b.rcell = w - x0 + 2;
-			}
-		}
+		b.bytes = 8u * BK_CELLS;
+		return b;
 	}
-	b.bytes = 8u * (unsigned)b.n + (b.lsrc != -1 ? 16u : 0u) + (b.rsrc != -1 ? 16u : 0u);
+	const long long ro = (long long)my * w;
+	const int a = x0 - 2 < 0 ? 0 : x0 - 2;
+	const int e = x0 + BK_COLS + 2 < w ? x0 + BK_COLS + 2 : w;
+	const int head = (int)((mis + ro + a) & 1); // element a is 8 bytes off a 16-byte boundary
+	const int a1 = a + head;
+	b.shift = a1 & 1; // cell of a1 (x0 is even) made even
+	const int len = e - a1 > 0 ? e - a1 : 0;
+	b.src = ro + a1;
+	b.cell = a1 - x0 + 2 + b.shift;
+	b.n = len & ~1;
+	b.bytes = 8u * (unsigned)b.n;
+	if (head) {
+		b.hsrc = ro + a;
+		b.hcell = a - x0 + 2 + b.shift;
+	}
+	if (len & 1) {
+		b.tsrc = ro + e - 1;
+		b.tcell = e - 1 - x0 + 2 + b.shift;
+	}
+	if (x0 == 0) { // column -1
+		const int mx = border_index(-1, w, lm);
+		b.lsrc = mx < 0 ? -1 : ro + mx;
+		b.lcell = 1 + b.shift;
+	}
+	if (w <= x0 + BK_COLS) { // column w
+		const int mx = border_index(w, w, lm);
+		b.rsrc = mx < 0 ? -1 : ro + mx;
+		b.rcell = w - x0 + 2 + b.shift;
+	}
 	return b;
 }
 
-// One warp per 32 x 32 block: floor = min over the block of max(error, 0),
-// with NaN counted as 0.
+// Floors of 32 x 32 blocks (see the head of this file); one warp per block,
+// one lane per column.  floors is the workspace's array; job.out indexes it.
 __global__ void __launch_bounds__(256)
-errfloor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
-	double *floors)
+floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
+	DetectParams prm, BlockFloor *floors)
 {
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	const double tmin2 = fmin(prm.thi2, prm.tlo2);
 	for (int j = gw; j < njobs; j += nw) {
 		const FloorJob jb = jobs[j];
 		const FrameDesc &fd = frames[jb.frame];
-		const int w = fd.w, x = jb.x0 + lane;
-		const int y1 = jb.y0 + FLOOR_BLOCK < fd.h ? jb.y0 + FLOOR_BLOCK : fd.h;
-		double m = INFINITY;
-		if (x < w)
-			for (int y = jb.y0; y < y1; ++y) {
-				const double v = fd.error[(long long)y * w + x];
-				m = dmin(m, v > 0 ? v : 0.0);
-			}
+		const int w = fd.w, h = fd.h, x = jb.x0 + lane;
+		const int n = (jb.y0 + FLOOR_BLOCK < h ? jb.y0 + FLOOR_BLOCK : h) - jb.y0;
+		const bool in = x < w;
+		const long long at = (long long)jb.y0 * w + x;
+		if (jb.kind == FLOOR_ERROR) {
+			double m = INFINITY;
+			if (in)
+#pragma unroll 8
+				for (int k = 0; k < n; ++k) {
+					const double v = fd.error[at + (long long)k * w];
+					m = dmin(m, v > 0 ? v : 0.0);
+				}
 #pragma unroll
-		for (int o = 16; o; o >>= 1)
-			m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-		if (lane == 0)
-			floors[jb.out] = m;
+			for (int o = 16; o; o >>= 1)
+				m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+			const double T = tmin2 * m;
+			if (lane == 0)
+				floors[jb.out].thr = T >= 0 ? T : 0.0; // NaN lists everything
+		} else {
+			unsigned long long key = ~0ull;
+			double gmax = fd.gain_map ? -INFINITY : fd.gain, rnmin = fd.rn_map ? INFINITY : fd.rn;
+			if (in)
+#pragma unroll 8
+				for (int k = 0; k < n; ++k) {
+					const long long i = at + (long long)k * w;
+					key = min(key, order_key(fd.clean[i]));
+					if (fd.gain_map)
+						gmax = dmax(gmax, fd.gain_map[i]);
+					if (fd.rn_map)
+						rnmin = dmin(rnmin, fd.rn_map[i]);
+				}
+#pragma unroll
+			for (int o = 16; o; o >>= 1) {
+				key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+				gmax = dmax(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+				rnmin = dmin(rnmin, __shfl_xor_sync(0xffffffffu, rnmin, o));
+			}
+			if (lane == 0)
+				floors[jb.out] = BlockFloor{0.0, key, gmax, rnmin};
+		}
 	}
 }
 
-// positive(v) on the sign bit: v if it is clear, +0 otherwise.
-__device__ __forceinline__ double pos_bits(double v)
+// Threshold of noise-model block (bx, by) of a bw x bh block grid from the
+// keys of its neighbourhood (see the head of this file).
+__device__ __forceinline__ int nbr_block(int b, int n, int i, bool wrap)
 {
-	const long long b = __double_as_longlong(v);
-	return __longlong_as_double(b & ~(b >> 63));
+	// i = 0..2: b - 1 .. b + 1; i = 3..6 (wrap mode near an edge only): the two
+	// blocks at each edge.  -1: none.
+	if (i < 3)
+		return b - 1 + i >= 0 && b - 1 + i < n ? b - 1 + i : -1;
+	if (!wrap || (b > 1 && b < n - 2))
+		return -1;
+	const int v = i == 3 ? 0 : i == 4 ? 1 : i == 5 ? n - 2 : n - 1;
+	return v >= 0 && v < n ? v : -1;
+}
+
+__device__ __forceinline__ double model_threshold(const BlockFloor *bf, int w, int h, int bx, int by,
+	int mode, double tmin2)
+{
+	const int bw = (w + FLOOR_BLOCK - 1) / FLOOR_BLOCK, bh = (h + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
+	const bool wrap = mode == WRAP;
+	unsigned long long key = ~0ull;
+	for (int i = 0; i < 7; ++i) {
+		const int yy = nbr_block(by, bh, i, wrap);
+		if (yy < 0)
+			continue;
+		for (int j = 0; j < 7; ++j) {
+			const int xx = nbr_block(bx, bw, j, wrap);
+			if (xx >= 0)
+				key = min(key, bf[yy * bw + xx].key);
+		}
+	}
+	// In constant mode a window reaching past the frame holds zeros.
+	if (mode == CONSTANT && (bx == 0 || by == 0 || (bx + 1) * FLOOR_BLOCK + 2 > w ||
+		(by + 1) * FLOOR_BLOCK + 2 > h))
+		key = min(key, order_key(0.0));
+	double m = order_value(key);
+	m = m < SIGNAL_FLOOR ? SIGNAL_FLOOR : m;
+	const BlockFloor &own = bf[by * bw + bx];
+	return tmin2 * (sqrt(own.rnmin * own.rnmin + own.gmax * m) / own.gmax);
+}
+
+// Upper bound of positive(v): v when its sign bit is clear; otherwise the
+// high word cleared (0 or a subnormal).
+__device__ __forceinline__ double pos_ub(double v)
+{
+	const int hi = __double2hiint(v);
+	return __hiloint2double(hi & ~(hi >> 31), __double2loint(v));
 }
 
 __device__ __forceinline__ unsigned hi_word(double v)
 {
-	return (unsigned)((unsigned long long)__double_as_longlong(v) >> 32);
+	return (unsigned)__double2hiint(v);
 }
 
-// Producer warp of sig_bulk_kernel: returns false after a fault.
+// Producer warp of sig_bulk_kernel; g counts the ring rows issued.  Returns
+// false after a fault.
 __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__restrict__ frames,
 	const FrameState *__restrict__ state, const int4 *__restrict__ items, int nitems, int lm,
 	Control *ctl, int &g)
@@ -259,10 +377,7 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 				const int4 it = items[cand];
 				if (!state[it.x].active)
 					continue;
-				const FrameDesc &fd = frames[it.x];
-				// The host lists only frames whose rows are 16-byte aligned;
-				// a descriptor that breaks this is reported, never copied.
-				if ((fd.w & 1) || ((uintptr_t)fd.clean & 15))
+				if ((uintptr_t)frames[it.x].clean & 7) // the host rejects such buffers
 					ok = false;
 				else
 					t = cand;
@@ -273,47 +388,56 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 			return false;
 		t = __shfl_sync(0xffffffffu, t, 0);
 		if (t < 0) { // end of the list: an end marker in the next ring row
+			const int slot = g & (BK_SLOTS - 1);
 			if (lane == 0) {
-				const int slot = g & (BK_SLOTS - 1);
 				ok = g < BK_SLOTS || mbar_wait(&R.empty[slot], ((g / BK_SLOTS) - 1) & 1, &R.abort);
 				if (ok) {
 					R.meta[slot] = make_int2(-1, 0);
 					mbar_arrive(&R.full[slot]);
-					++g;
+					mbar_arrive(&R.full[slot]);
 				}
 			}
-			return __shfl_sync(0xffffffffu, ok, 0);
+			ok = __shfl_sync(0xffffffffu, ok, 0);
+			g += ok;
+			return ok;
 		}
 		const int4 it = items[t];
 		const FrameDesc &fd = frames[it.x];
 		const int w = fd.w, h = fd.h, words = fd.words, x0 = it.y, y0 = it.z;
 		const int y1 = y0 + BK_ROWS < h ? y0 + BK_ROWS : h;
 		const double *clean = fd.clean;
+		const int mis = (int)(((uintptr_t)clean >> 3) & 1);
 		uint32_t *s1 = plane_ptr(fd, P_S1);
 		const long long plane = fd.plane;
 		for (int r = y0 - 1; r <= y1; ++r) {
-			if (lane == 0) {
-				const int slot = g & (BK_SLOTS - 1);
+			const int slot = g & (BK_SLOTS - 1);
+			if (lane == 0)
 				ok = g < BK_SLOTS || mbar_wait(&R.empty[slot], ((g / BK_SLOTS) - 1) & 1, &R.abort);
-				if (ok) {
-					if (r == y0 - 1)
-						R.meta[slot] = make_int2(t, y1);
-					const BulkRow b = bulk_row(w, h, lm, x0, r);
-					unsigned long long *bar = &R.full[slot];
-					mbar_expect_tx(bar, b.bytes);
-					bulk_copy(&R.c[slot][b.cell], b.src < 0 ? bulk_zero_row : clean + b.src,
-						8u * b.n, bar);
-					if (b.lsrc != -1)
-						bulk_copy(&R.c[slot][0], b.lsrc < 0 ? bulk_zero_row : clean + b.lsrc, 16u,
-							bar);
-					if (b.rsrc != -1)
-						bulk_copy(&R.c[slot][b.rcell], b.rsrc < 0 ? bulk_zero_row : clean + b.rsrc,
-							16u, bar);
-					++g;
-				}
-			}
 			if (!__shfl_sync(0xffffffffu, ok, 0))
 				return false;
+			__syncwarp();
+			const BulkRow b = bulk_row(w, h, lm, mis, x0, r);
+			double *row = R.c[slot];
+			if (lane == 0) {
+				if (r == y0 - 1)
+					R.meta[slot] = make_int2(t, y1);
+				R.shift[slot] = b.shift;
+				mbar_expect_tx(&R.full[slot], b.bytes);
+				if (b.n)
+					bulk_copy(row + b.cell, b.src < 0 ? bulk_zero_row : clean + b.src, 8u * b.n,
+						&R.full[slot]);
+			} else if (lane == 1) {
+				if (b.hsrc != NO_COPY)
+					cp_async8(row + b.hcell, clean + b.hsrc);
+				if (b.tsrc != NO_COPY)
+					cp_async8(row + b.tcell, clean + b.tsrc);
+				if (b.lsrc != NO_COPY)
+					cp_async8(row + b.lcell, b.lsrc < 0 ? bulk_zero_row : clean + b.lsrc);
+				if (b.rsrc != NO_COPY)
+					cp_async8(row + b.rcell, b.rsrc < 0 ? bulk_zero_row : clean + b.rsrc);
+				mbar_arrive_cp_async(&R.full[slot]);
+			}
+			++g;
 			// Clear the S1, S2 and CAND words of the item's rows (16 words per
 			// plane per row).
 			if (r >= y0 && r < y1)
@@ -326,15 +450,35 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 	}
 }
 
+// Columns x - 1 .. x + 2 of a ring row (x = the pair's first column, at cell
+// c + shift; c even, so every 16-byte load is aligned).
+__device__ __forceinline__ void load_quad(const double *row, int c, int shift, double &l, double &a,
+	double &b, double &r)
+{
+	if (shift == 0) {
+		const double2 v = *reinterpret_cast<const double2 *>(row + c);
+		l = row[c - 1];
+		a = v.x;
+		b = v.y;
+		r = row[c + 2];
+	} else {
+		const double2 v0 = *reinterpret_cast<const double2 *>(row + c);
+		const double2 v1 = *reinterpret_cast<const double2 *>(row + c + 2);
+		l = v0.x;
+		a = v0.y;
+		b = v1.x;
+		r = v1.y;
+	}
+}
+
 // Consumer warps of sig_bulk_kernel: returns false after a fault.
 __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__restrict__ frames,
-	const int4 *__restrict__ items, const double *__restrict__ floors, const DetectParams &prm,
-	int lm, PreCand *pre, int *pre_counts)
+	const int4 *__restrict__ items, const DetectParams &prm, PreCand *pre, int *pre_counts)
 {
+	const double tmin2 = fmin(prm.thi2, prm.tlo2);
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int ct = warp * 32 + lane; // 0 .. 127
 	const unsigned below = (1u << lane) - 1u;
-	const double tmin2 = fmin(prm.thi2, prm.tlo2);
 	int g = 0;
 	bool ok = true;
 	for (;;) {
@@ -347,65 +491,81 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 		const int t = meta.x, y1 = meta.y;
 		const int4 it = items[t];
 		const int f = it.x, x0 = it.y, y0 = it.z;
-		const int w = frames[f].w;
+		const FrameDesc &fd = frames[f];
+		const int w = fd.w, by = y0 / FLOOR_BLOCK;
 		const int bw = (w + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
-		const double *frow = floors + it.w + (long long)(y0 / FLOOR_BLOCK) * bw;
 		// Pair sets p = 0, 1: columns xs[p] = x0 + 256 p + 2 ct and xs[p] + 1.
 		int xs[2];
-		bool nl[2], nr[2];
-		unsigned thr[2];
+		unsigned ta[2], tb[2]; // high word of the block threshold (all ones: not a pixel)
 #pragma unroll
 		for (int p = 0; p < 2; ++p) {
 			xs[p] = x0 + BK_HALF * p + 2 * ct;
-			const bool valid = xs[p] < w;
-			nl[p] = lm == NEAREST && xs[p] == 0;
-			nr[p] = lm == NEAREST && xs[p] + 2 == w;
-			double T = valid ? tmin2 * frow[xs[p] / FLOOR_BLOCK] : 0.0;
-			T = T >= 0 ? T : 0.0; // NaN (0 x inf) lists everything
-			thr[p] = valid ? hi_word(T) : 0xffffffffu;
+			ta[p] = 0xffffffffu;
+			if (xs[p] < w) {
+				const int bx = xs[p] / FLOOR_BLOCK;
+				double T = fd.error ? fd.floors[by * bw + bx].thr
+					: model_threshold(fd.floors, w, fd.h, bx, by, prm.mode, tmin2);
+				ta[p] = hi_word(T >= 0 ? T : 0.0); // NaN lists everything
+			}
+			tb[p] = xs[p] + 1 < w ? ta[p] : 0xffffffffu;
 		}
 		ok = __all_sync(0xffffffffu,
 			mbar_wait(&R.full[(g + 1) & (BK_SLOTS - 1)], ((g + 1) / BK_SLOTS) & 1, &R.abort));
 		if (!ok)
 			break;
-		double qa[2], qb[2], upa[2], upb[2];
+		// Row y0 - 1 (pair values) and row y0 (pair values and neighbours).
+		double qa[2], qb[2], ql[2], qr[2], upa[2], upb[2];
+		{
+			const int su = R.shift[g & (BK_SLOTS - 1)], sc = R.shift[(g + 1) & (BK_SLOTS - 1)];
+			const double *ru = R.c[g & (BK_SLOTS - 1)], *rc = R.c[(g + 1) & (BK_SLOTS - 1)];
 #pragma unroll
-		for (int p = 0; p < 2; ++p) {
-			const int cell = 2 + BK_HALF * p + 2 * ct;
-			const double2 u = *reinterpret_cast<const double2 *>(&R.c[g & (BK_SLOTS - 1)][cell]);
-			const double2 c = *reinterpret_cast<const double2 *>(&R.c[(g + 1) & (BK_SLOTS - 1)][cell]);
-			qa[p] = c.x * 0.25;
-			qb[p] = c.y * 0.25;
-			upa[p] = qa[p] - u.x * 0.25;
-			upb[p] = qb[p] - u.y * 0.25;
+			for (int p = 0; p < 2; ++p) {
+				const int c = 2 + BK_HALF * p + 2 * ct;
+				double ul, ua, ub, ur;
+				load_quad(ru, c, su, ul, ua, ub, ur);
+				load_quad(rc, c, sc, ql[p], qa[p], qb[p], qr[p]);
+				qa[p] *= 0.25;
+				qb[p] *= 0.25;
+				ql[p] *= 0.25;
+				qr[p] *= 0.25;
+				upa[p] = qa[p] - ua * 0.25;
+				upb[p] = qb[p] - ub * 0.25;
+			}
 		}
 		__syncwarp();
-		if (lane == 0)
-			mbar_arrive(&R.empty[g & (BK_SLOTS - 1)]); // row y0 - 1
+		if (lane == 0) { // both rows are in registers now
+			mbar_arrive(&R.empty[g & (BK_SLOTS - 1)]);
+			mbar_arrive(&R.empty[(g + 1) & (BK_SLOTS - 1)]);
+		}
 		PreCand *region = pre + ((long long)t * BK_CWARPS + warp) * BK_REGION;
 		int cnt = 0;
 		for (int y = y0; y < y1; ++y) {
-			const int gd = g + 2 + (y - y0); // ring rows of y + 1 (gd) and y (gd - 1)
-			const int sd = gd & (BK_SLOTS - 1), sc = (gd - 1) & (BK_SLOTS - 1);
+			const int gd = g + 2 + (y - y0); // ring row of y + 1
+			const int sd = gd & (BK_SLOTS - 1);
 			ok = __all_sync(0xffffffffu, mbar_wait(&R.full[sd], (gd / BK_SLOTS) & 1, &R.abort));
 			if (!ok)
 				break;
+			double nl[2], na[2], nb[2], nr[2];
+			{
+				const int s = R.shift[sd];
+#pragma unroll
+				for (int p = 0; p < 2; ++p)
+					load_quad(R.c[sd], 2 + BK_HALF * p + 2 * ct, s, nl[p], na[p], nb[p], nr[p]);
+			}
+			__syncwarp();
+			if (lane == 0)
+				mbar_arrive(&R.empty[sd]); // row y + 1 is in registers
 			const long long rowpix = (long long)y * w;
 #pragma unroll
 			for (int p = 0; p < 2; ++p) {
-				const int cell = 2 + BK_HALF * p + 2 * ct;
-				const double2 dn = *reinterpret_cast<const double2 *>(&R.c[sd][cell]);
-				double ql = R.c[sc][cell - 1] * 0.25, qr = R.c[sc][cell + 2] * 0.25;
-				ql = nl[p] ? qa[p] : ql;
-				qr = nr[p] ? qb[p] : qr;
-				const double qda = dn.x * 0.25, qdb = dn.y * 0.25;
+				const double qda = na[p] * 0.25, qdb = nb[p] * 0.25;
 				const double da = qa[p] - qda, db = qb[p] - qdb;
-				const double hl = qa[p] - ql, hab = qa[p] - qb[p], hr = qb[p] - qr;
-				const double lap_a = (pos_bits(upa[p] + hl) + pos_bits(upa[p] + hab)) +
-					(pos_bits(da + hl) + pos_bits(da + hab));
-				const double lap_b = (pos_bits(upb[p] - hab) + pos_bits(upb[p] + hr)) +
-					(pos_bits(db - hab) + pos_bits(db + hr));
-				const bool pa = hi_word(lap_a) >= thr[p], pb = hi_word(lap_b) >= thr[p];
+				const double hl = qa[p] - ql[p], hab = qa[p] - qb[p], hr = qb[p] - qr[p];
+				const double lap_a = (pos_ub(upa[p] + hl) + pos_ub(upa[p] + hab)) +
+					(pos_ub(da + hl) + pos_ub(da + hab));
+				const double lap_b = (pos_ub(upb[p] - hab) + pos_ub(upb[p] + hr)) +
+					(pos_ub(db - hab) + pos_ub(db + hr));
+				const bool pa = hi_word(lap_a) >= ta[p], pb = hi_word(lap_b) >= tb[p];
 				const unsigned ba = __ballot_sync(0xffffffffu, pa);
 				if (ba) {
 					if (pa)
@@ -424,18 +584,14 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 				upb[p] = -db;
 				qa[p] = qda;
 				qb[p] = qdb;
+				ql[p] = nl[p] * 0.25;
+				qr[p] = nr[p] * 0.25;
 			}
-			__syncwarp();
-			if (lane == 0)
-				mbar_arrive(&R.empty[sc]); // row y
 		}
 		if (!ok)
 			break;
-		__syncwarp();
-		if (lane == 0) {
-			mbar_arrive(&R.empty[(g + y1 - y0 + 1) & (BK_SLOTS - 1)]); // row y1
+		if (lane == 0)
 			pre_counts[t * BK_CWARPS + warp] = cnt;
-		}
 		g += y1 - y0 + 2;
 	}
 	return ok;
@@ -443,28 +599,26 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 
 __global__ void __launch_bounds__(BK_THREADS, BK_BLOCKS_PER_SM)
 sig_bulk_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
-	const int4 *__restrict__ items, int nitems, const double *__restrict__ floors,
-	DetectParams prm, Control *ctl, PreCand *pre, int *pre_counts)
+	const int4 *__restrict__ items, int nitems, DetectParams prm, Control *ctl, PreCand *pre,
+	int *pre_counts)
 {
 	__shared__ BulkRing R;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	const int lm = lap_mode(prm.mode);
 	if (tid == 0) {
 		for (int i = 0; i < BK_SLOTS; ++i) {
-			mbar_init(&R.full[i], 1);
+			mbar_init(&R.full[i], 2); // producer lanes 0 (bytes) and 1 (cp.async)
 			mbar_init(&R.empty[i], BK_CWARPS);
 		}
 		R.abort = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 	}
 	__syncthreads();
-
-	bool ok = true;
-	int issued = 0; // ring rows issued (producer lane 0)
+	bool ok;
+	int issued = 0; // ring rows issued (producer warp)
 	if (warp == BK_CWARPS)
-		ok = bulk_producer(R, frames, state, items, nitems, lm, ctl, issued);
+		ok = bulk_producer(R, frames, state, items, nitems, lap_mode(prm.mode), ctl, issued);
 	else
-		ok = bulk_consumer(R, frames, items, floors, prm, lm, pre, pre_counts);
+		ok = bulk_consumer(R, frames, items, prm, pre, pre_counts);
 	if (!ok && lane == 0) {
 		R.abort = 1;
 		atomicOr(&ctl->fault, 1);
@@ -482,55 +636,120 @@ sig_bulk_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 		}
 }
 
-// Exact sig_raw of the listed pixels (src/filters.cuh:125-135, lap / (2 *
-// noise)): one warp per consumer-warp region of an item, one lane per entry;
-// the high list grows from the front of the candidate buffer, the low list
-// from its back.
+// Candidates staged in shared memory by classify_kernel before one global
+// append per block and list.
+constexpr int CL_CAP = 1024;
+
+struct ClassifyStage {
+	uint2 buf[CL_CAP];
+	int n;    // slots reserved
+	int fail; // first reservation that did not fit (entries from there went straight out)
+};
+
+// Stage the lanes whose `pred` holds (entry e); a reservation that does not
+// fit appends those entries to the global list directly.
+__device__ __forceinline__ void classify_stage(ClassifyStage &S, bool pred, uint2 e,
+	unsigned long long *counter, uint2 *cands, bool from_back, unsigned long long cap)
+{
+	const int lane = threadIdx.x & 31;
+	const unsigned b = __ballot_sync(0xffffffffu, pred);
+	if (!b)
+		return;
+	const int k = __popc(b), rank = __popc(b & ((1u << lane) - 1u));
+	int old = 0;
+	if (lane == 0)
+		old = atomicAdd(&S.n, k);
+	old = __shfl_sync(0xffffffffu, old, 0);
+	if (old + k <= CL_CAP) {
+		if (pred)
+			S.buf[old + rank] = e;
+		return;
+	}
+	unsigned long long base = 0;
+	if (lane == 0) {
+		atomicMin(&S.fail, old);
+		base = atomicAdd(counter, (unsigned long long)k);
+	}
+	base = __shfl_sync(0xffffffffu, base, 0);
+	if (pred)
+		cands[from_back ? cap - 1 - (base + rank) : base + rank] = e;
+}
+
+// Write a stage out with one atomic per list (block-uniform call).
+__device__ __forceinline__ void classify_flush(ClassifyStage &H, ClassifyStage &L, Control *ctl,
+	uint2 *cands, unsigned long long *bases)
+{
+	__syncthreads();
+	const int nh = min(H.n, H.fail), nl = min(L.n, L.fail);
+	if (threadIdx.x == 0) {
+		bases[0] = nh ? atomicAdd(&ctl->n_cand, (unsigned long long)nh) : 0ull;
+		bases[1] = nl ? atomicAdd(&ctl->n_low, (unsigned long long)nl) : 0ull;
+	}
+	__syncthreads();
+	const unsigned long long cap = ctl->cand_cap;
+	for (int i = threadIdx.x; i < nh; i += blockDim.x)
+		cands[bases[0] + i] = H.buf[i];
+	for (int i = threadIdx.x; i < nl; i += blockDim.x)
+		cands[cap - 1 - (bases[1] + i)] = L.buf[i];
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		H.n = L.n = 0;
+		H.fail = L.fail = CL_CAP;
+	}
+	__syncthreads();
+}
+
+// sig_raw of the listed pixels, lap / (2 noise) (src/filters.cuh:125-135),
+// with the error map or the exact noise model at the pixel: one warp per
+// consumer-warp region of an item, one lane per entry.  The high list grows
+// from the front of the candidate buffer, the low list from its back; a NaN
+// goes to the high list (the candidate kernel decides).
 __global__ void __launch_bounds__(256)
 classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const int4 *__restrict__ items, int nitems, const PreCand *__restrict__ pre,
 	const int *__restrict__ pre_counts, DetectParams prm, Control *ctl, uint2 *cands)
 {
-	const int lane = threadIdx.x & 31;
-	const unsigned below = (1u << lane) - 1u;
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	__shared__ ClassifyStage H, L;
+	__shared__ unsigned long long bases[2];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (threadIdx.x == 0) {
+		H.n = L.n = 0;
+		H.fail = L.fail = CL_CAP;
+	}
+	__syncthreads();
+	const unsigned long long cap = ctl->cand_cap;
 	const int nreg = nitems * BK_CWARPS;
-	for (int rg = gw; rg < nreg; rg += nw) {
-		const int f = items[rg / BK_CWARPS].x;
-		if (!state[f].active)
-			continue; // warp-uniform: the region was not written this pass
-		const int n = pre_counts[rg];
-		const double *error = frames[f].error;
-		const PreCand *e = pre + (long long)rg * BK_REGION;
-		for (int k0 = 0; k0 < n; k0 += 32) {
-			int cls = 0;
-			unsigned pix = 0;
-			if (k0 + lane < n) {
-				const PreCand pc = e[k0 + lane];
-				pix = pc.pixel;
-				const double v = pc.lap / (2 * error[pc.pixel]);
-				cls = v > prm.cr ? 1 : v > prm.nb ? 2 : 0;
-			}
-			const unsigned bh = __ballot_sync(0xffffffffu, cls == 1);
-			const unsigned bl = __ballot_sync(0xffffffffu, cls == 2);
-			if (bh) {
-				unsigned long long base = 0;
-				if (lane == 0)
-					base = atomicAdd(&ctl->n_cand, (unsigned long long)__popc(bh));
-				base = __shfl_sync(0xffffffffu, base, 0);
-				if (cls == 1)
-					cands[base + __popc(bh & below)] = make_uint2((unsigned)f, pix);
-			}
-			if (bl) {
-				unsigned long long base = 0;
-				if (lane == 0)
-					base = atomicAdd(&ctl->n_low, (unsigned long long)__popc(bl));
-				base = __shfl_sync(0xffffffffu, base, 0);
-				if (cls == 2)
-					cands[ctl->cand_cap - 1 - (base + __popc(bl & below))] = make_uint2((unsigned)f, pix);
+	for (int base = blockIdx.x * 8; base < nreg; base += gridDim.x * 8) { // block-uniform
+		const int rg = base + warp;
+		const int f = rg < nreg ? items[rg / BK_CWARPS].x : 0;
+		if (rg < nreg && state[f].active) { // warp-uniform
+			const int n = pre_counts[rg];
+			const FrameDesc &fd = frames[f];
+			const PreCand *e = pre + (long long)rg * BK_REGION;
+			for (int k0 = 0; k0 < n; k0 += 32) {
+				int cls = 0;
+				unsigned pix = 0;
+				if (k0 + lane < n) {
+					const PreCand pc = e[k0 + lane];
+					pix = pc.pixel;
+					const double nz = fd.error ? fd.error[pix]
+						: noise_model_at(fd, (int)(pix % (unsigned)fd.w), (int)(pix / (unsigned)fd.w),
+							prm.mode);
+					const double v = pc.lap / (2 * nz);
+					cls = v > prm.cr || v != v ? 1 : v > prm.nb ? 2 : 0;
+				}
+				const uint2 entry = make_uint2((unsigned)f, pix);
+				classify_stage(H, cls == 1, entry, &ctl->n_cand, cands, false, cap);
+				classify_stage(L, cls == 2, entry, &ctl->n_low, cands, true, cap);
 			}
 		}
+		__syncthreads();
+		const bool full = H.n >= CL_CAP / 2 || L.n >= CL_CAP / 2;
+		__syncthreads(); // every thread has read the counts before any stages again
+		if (full)
+			classify_flush(H, L, ctl, cands, bases);
 	}
+	classify_flush(H, L, ctl, cands, bases);
 }
 
 } // namespace cb

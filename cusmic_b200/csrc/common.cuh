@@ -71,6 +71,16 @@ CB_HD int clampi(int x, int lo, int hi)
 	return x < lo ? lo : x > hi ? hi : x;
 }
 
+// Noise floor of a 32 x 32 block of a frame (see bulk.cuh): the detection
+// threshold of an error-map block, or for a noise-model block a lower bound of
+// its clean values (as an ordered key, lowered by every replacement inside
+// the block) with the block's largest gain and smallest read noise.
+struct BlockFloor {
+	double thr;
+	unsigned long long key;
+	double gmax, rnmin;
+};
+
 // One frame of a (possibly ragged) batch, as the kernels see it.
 struct FrameDesc {
 	const double *data, *error, *gain_map, *rn_map, *bg_map;
@@ -78,6 +88,7 @@ struct FrameDesc {
 	double *clean;     // working pixels, restored in place into the output
 	uint8_t *mask_out; // uint8 output mask
 	uint32_t *bits;    // N_PLANES planes of `plane` words
+	BlockFloor *floors; // the frame's block floors, row-major by block (null: none)
 	double gain, rn, bg;
 	long long plane;   // words per plane = h * words
 	int w, h, words, has_bg;

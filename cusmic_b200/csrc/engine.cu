@@ -100,12 +100,10 @@ template <class T> struct PinBuf {
 struct Layout {
 	std::vector<FrameDesc> frames;
 	std::vector<long long> bit_off; // word offset of each frame's planes
-	std::vector<int4> tiles; // sig_model_kernel tiles (noise-model frames)
-	std::vector<int4> strips; // sig_stream_kernel items (error-map frames, other layouts)
-	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, floor base} (see bulk_eligible)
-	std::vector<FloorJob> floor_jobs; // 32 x 32 blocks of each distinct error map of bulk frames
-	std::vector<long long> floor_base; // per frame: first floor of its map (-1: none)
-	long long nfloors = 0;
+	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, first threshold of the frame}
+	std::vector<FloorJob> jobs; // floor blocks: of each distinct error map, of each noise-model frame
+	std::vector<long long> thr_base; // per frame: first floor of its blocks
+	long long nthr = 0;
 	std::vector<int2> rows;
 	std::vector<long long> offsets; // first output pixel of each frame
 	long long total_words = 0;
@@ -135,16 +133,14 @@ struct Workspace {
 	int device = -1;
 	DevBuf<FrameDesc> frames;
 	DevBuf<FrameState> state;
-	DevBuf<int4> tiles;
 	DevBuf<int2> rows;
 	DevBuf<uint32_t> bits;
 	DevBuf<uint2> targets;
 	DevBuf<uint2> cands;
 	DevBuf<Seed> seeds;
-	DevBuf<int4> strips;
 	DevBuf<int4> bulk;
-	DevBuf<FloorJob> fjobs;
-	DevBuf<double> floors;
+	DevBuf<FloorJob> jobs;
+	DevBuf<BlockFloor> floors;
 	DevBuf<PreCand> pre;
 	DevBuf<int> pre_counts;
 	DevBuf<Control> ctl;
@@ -244,14 +240,16 @@ static void check_arguments(const cusmic_image *ims, size_t nf, const cusmic_opt
 	}
 }
 
-// The bulk detection kernel copies whole row segments of clean and of the
-// error map with cp.async.bulk, which needs 16-byte aligned addresses and
-// sizes: both buffers 16-byte aligned and an even width (so every row of both
-// starts on a 16-byte boundary).
-static bool bulk_eligible(const FrameDesc &d)
+// Device buffers hold float64 values: every pointer must be 8-byte aligned.
+static void check_device_alignment(const cusmic_image *ims, size_t nf, const double *clean)
 {
-	return d.error && d.w % 2 == 0 && ((uintptr_t)d.clean & 15) == 0 &&
-		((uintptr_t)d.error & 15) == 0;
+	auto bad = [](const void *p) { return ((uintptr_t)p & 7) != 0; };
+	bool any = bad(clean);
+	for (size_t f = 0; f < nf; ++f)
+		any = any || bad(ims[f].data) || bad(ims[f].error) || bad(ims[f].gain) ||
+			bad(ims[f].readnoise) || bad(ims[f].background);
+	if (any)
+		throw InvalidArgument("float64 buffers must be 8-byte aligned");
 }
 
 static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
@@ -268,7 +266,7 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 	L.prm.mode = o.border;
 	L.frames.resize(nf);
 	L.bit_off.resize(nf);
-	L.floor_base.assign(nf, -1);
+	L.thr_base.assign(nf, -1);
 	std::map<const double *, std::vector<std::pair<int, long long>>> maps; // error map -> {frame, base}
 	size_t px = 0;
 	long long words = 0;
@@ -299,38 +297,30 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		px += (size_t)d.w * d.h;
 		for (int y = 0; y < d.h; ++y)
 			L.rows.push_back(make_int2((int)f, y));
-		if (d.error && bulk_eligible(d)) {
-			// Frames of the same shape that share an error map share its floors.
-			long long base = -1;
+		// Thresholds: frames of the same shape that share an error map share
+		// them; every noise-model frame has its own.
+		const int bw = (d.w + FLOOR_BLOCK - 1) / FLOOR_BLOCK, bh = (d.h + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
+		long long base = -1;
+		if (d.error)
 			for (const auto &m : maps[d.error])
 				if (L.frames[m.first].w == d.w && L.frames[m.first].h == d.h)
 					base = m.second;
-			if (base < 0) {
-				base = L.nfloors;
+		if (base < 0) {
+			base = L.nthr;
+			if (d.error)
 				maps[d.error].push_back({(int)f, base});
-				const int bw = (d.w + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
-				const int bh = (d.h + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
-				for (int by = 0; by < bh; ++by)
-					for (int bx = 0; bx < bw; ++bx)
-						L.floor_jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK, 0,
-							base + (long long)by * bw + bx});
-				L.nfloors += (long long)bw * bh;
-			}
-			if (base > INT_MAX)
-				throw std::bad_alloc();
-			L.floor_base[f] = base;
-			for (int ty = 0; ty < d.h; ty += BK_ROWS)
-				for (int tx = 0; tx < d.w; tx += BK_COLS)
-					L.bulk.push_back(make_int4((int)f, tx, ty, (int)base));
-		} else if (d.error) {
-			for (int ty = 0; ty < d.h; ty += STREAM_ROWS)
-				for (int tx = 0; tx < d.w; tx += 32)
-					L.strips.push_back(make_int4((int)f, tx, ty, 0));
-		} else {
-			for (int ty = 0; ty < d.h; ty += MTILE)
-				for (int tx = 0; tx < d.w; tx += MTILE)
-					L.tiles.push_back(make_int4((int)f, tx, ty, 0));
+			for (int by = 0; by < bh; ++by)
+				for (int bx = 0; bx < bw; ++bx)
+					L.jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK,
+						d.error ? FLOOR_ERROR : FLOOR_MODEL, base + (long long)by * bw + bx});
+			L.nthr += (long long)bw * bh;
 		}
+		if (base > INT_MAX)
+			throw std::bad_alloc();
+		L.thr_base[f] = base;
+		for (int ty = 0; ty < d.h; ty += BK_ROWS)
+			for (int tx = 0; tx < d.w; tx += BK_COLS)
+				L.bulk.push_back(make_int4((int)f, tx, ty, (int)base));
 	}
 	L.total_px = px;
 	L.total_words = words;
@@ -350,15 +340,9 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	const size_t nf = L.frames.size();
 	ws.frames.ensure(nf);
 	ws.state.ensure(nf);
-	ws.tiles.ensure(L.tiles.size() ? L.tiles.size() : 1);
-	ws.strips.ensure(L.strips.size() ? L.strips.size() : 1);
 	ws.bulk.ensure(L.bulk.size() ? L.bulk.size() : 1);
-	ws.fjobs.ensure(L.floor_jobs.size() ? L.floor_jobs.size() : 1);
-	ws.floors.ensure(L.nfloors ? (size_t)L.nfloors : 1);
-	if (L.maxiter && !L.bulk.empty()) {
-		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
-		ws.pre_counts.ensure(L.bulk.size() * BK_CWARPS);
-	}
+	ws.jobs.ensure(L.jobs.size() ? L.jobs.size() : 1);
+	ws.floors.ensure(L.nthr ? (size_t)L.nthr : 1);
 	ws.rows.ensure(L.rows.size());
 	ws.ctl.ensure(1);
 	ws.offsets.ensure(nf);
@@ -367,40 +351,40 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 		ws.targets.ensure(L.total_px);
 		ws.cands.ensure(L.total_px);
 		ws.seeds.ensure(L.total_px);
+		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
+		ws.pre_counts.ensure(L.bulk.size() * BK_CWARPS);
 	}
-	for (size_t f = 0; f < nf; ++f)
+	for (size_t f = 0; f < nf; ++f) {
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
-	size_t bytes_f = nf * sizeof(FrameDesc), bytes_t = L.tiles.size() * sizeof(int4);
-	size_t bytes_s = L.strips.size() * sizeof(int4), bytes_r = L.rows.size() * sizeof(int2);
-	size_t bytes_b = L.bulk.size() * sizeof(int4), bytes_j = L.floor_jobs.size() * sizeof(FloorJob);
-	ws.stage.ensure(bytes_f + bytes_t + bytes_s + bytes_r + bytes_b + bytes_j);
-	// The previous call using this workspace synchronised before returning,
-	// so the staging buffer is free.
-	unsigned char *st = ws.stage.p;
-	std::memcpy(st, L.frames.data(), bytes_f);
-	std::memcpy(st + bytes_f, L.tiles.data(), bytes_t);
-	std::memcpy(st + bytes_f + bytes_t, L.strips.data(), bytes_s);
-	std::memcpy(st + bytes_f + bytes_t + bytes_s, L.rows.data(), bytes_r);
-	std::memcpy(st + bytes_f + bytes_t + bytes_s + bytes_r, L.bulk.data(), bytes_b);
-	std::memcpy(st + bytes_f + bytes_t + bytes_s + bytes_r + bytes_b, L.floor_jobs.data(), bytes_j);
-	check(cudaMemcpyAsync(ws.frames.p, st, bytes_f, cudaMemcpyHostToDevice, s));
-	if (bytes_t)
-		check(cudaMemcpyAsync(ws.tiles.p, st + bytes_f, bytes_t, cudaMemcpyHostToDevice, s));
-	if (bytes_s)
-		check(cudaMemcpyAsync(ws.strips.p, st + bytes_f + bytes_t, bytes_s,
-			cudaMemcpyHostToDevice, s));
-	check(cudaMemcpyAsync(ws.rows.p, st + bytes_f + bytes_t + bytes_s, bytes_r,
-		cudaMemcpyHostToDevice, s));
-	if (bytes_b)
-		check(cudaMemcpyAsync(ws.bulk.p, st + bytes_f + bytes_t + bytes_s + bytes_r, bytes_b,
-			cudaMemcpyHostToDevice, s));
-	if (bytes_j)
-		check(cudaMemcpyAsync(ws.fjobs.p, st + bytes_f + bytes_t + bytes_s + bytes_r + bytes_b,
-			bytes_j, cudaMemcpyHostToDevice, s));
-	// Offsets are only read by the adjoint; a synchronous copy is fine.
-	check(cudaStreamSynchronize(s));
-	check(cudaMemcpy(ws.offsets.p, L.offsets.data(), nf * sizeof(long long),
-		cudaMemcpyHostToDevice));
+		L.frames[f].floors = L.maxiter ? ws.floors.p + L.thr_base[f] : nullptr;
+	}
+	// Every descriptor array goes through one pinned staging buffer.  The
+	// previous call using this workspace synchronised before returning, so
+	// the buffer is free.
+	struct Part {
+		void *dst;
+		const void *src;
+		size_t bytes;
+	};
+	const Part parts[] = {
+		{ws.frames.p, L.frames.data(), nf * sizeof(FrameDesc)},
+		{ws.rows.p, L.rows.data(), L.rows.size() * sizeof(int2)},
+		{ws.bulk.p, L.bulk.data(), L.bulk.size() * sizeof(int4)},
+		{ws.jobs.p, L.jobs.data(), L.jobs.size() * sizeof(FloorJob)},
+		{ws.offsets.p, L.offsets.data(), nf * sizeof(long long)},
+	};
+	size_t total = 0;
+	for (const Part &q : parts)
+		total += (q.bytes + 15) & ~size_t(15);
+	ws.stage.ensure(total);
+	size_t at = 0;
+	for (const Part &q : parts) {
+		if (q.bytes) {
+			std::memcpy(ws.stage.p + at, q.src, q.bytes);
+			check(cudaMemcpyAsync(q.dst, ws.stage.p + at, q.bytes, cudaMemcpyHostToDevice, s));
+		}
+		at += (q.bytes + 15) & ~size_t(15);
+	}
 }
 
 struct GraphLoop {
@@ -448,29 +432,14 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	const GraphLoop &gl, Recorder *rec = nullptr)
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
-	const int ntiles = (int)L.tiles.size(), nstrips = (int)L.strips.size();
 	const int nbulk = (int)L.bulk.size();
-	if (nbulk) {
-		const int cap = di.sms * BK_BLOCKS_PER_SM;
-		sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
-			ws.bulk.p, nbulk, ws.floors.p, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
-		mark(rec, K_SIGRAW);
-		classify_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk,
-			ws.pre.p, ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
-		mark(rec, K_CLASSIFY);
-	}
-	if (nstrips) {
-		int blocks = (nstrips + 7) / 8, cap = di.sms * 8;
-		sig_stream_kernel<<<blocks < cap ? blocks : cap, 256, 0, s>>>(ws.frames.p, ws.state.p,
-			ws.strips.p, nstrips, L.prm, ws.ctl.p, ws.cands.p);
-	}
-	if (ntiles) {
-		int cap = di.sms * 8;
-		sig_model_kernel<<<ntiles < cap ? ntiles : cap, 256, 0, s>>>(ws.frames.p, ws.state.p,
-			ws.tiles.p, ntiles, L.prm, ws.ctl.p, ws.cands.p);
-	}
-	if (nstrips || ntiles)
-		mark(rec, K_SIGRAW);
+	const int cap = di.sms * BK_BLOCKS_PER_SM;
+	sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
+		ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
+	mark(rec, K_SIGRAW);
+	classify_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
+		ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
+	mark(rec, K_CLASSIFY);
 	candidate_kernel<false><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
 		ws.seeds.p);
 	mark(rec, K_CAND);
@@ -496,12 +465,6 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
 		(unsigned long long)L.total_px);
 	mark(rec, K_INIT);
-	if (L.maxiter && !L.floor_jobs.empty()) {
-		const int nj = (int)L.floor_jobs.size(), cap = di.sms * 8;
-		errfloor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p,
-			ws.fjobs.p, nj, ws.floors.p);
-		mark(rec, K_FLOOR);
-	}
 	if (!L.maxiter) {
 		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
 		mark(rec, K_COPY);
@@ -513,6 +476,13 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
 		&ws.ctl.p->n_holes, 1);
 	mark(rec, K_FILL);
+	// Block floors of the filled frames (replacement keeps them lower bounds).
+	if (!L.jobs.empty()) {
+		const int nj = (int)L.jobs.size(), cap = di.sms * 8;
+		floor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p, ws.jobs.p,
+			nj, L.prm, ws.floors.p);
+		mark(rec, K_FLOOR);
+	}
 }
 
 static void launch_epilogue(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
@@ -597,6 +567,7 @@ static void run_device(const cusmic_image *ims, size_t nf, const cusmic_options 
 	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask, cudaStream_t s,
 	std::vector<int> *passes = nullptr)
 {
+	check_device_alignment(ims, nf, clean);
 	int dev;
 	check(cudaGetDevice(&dev));
 	DeviceInfo di = device_info(dev);
@@ -812,6 +783,7 @@ extern "C" int cusmic_plan_create(cusmic_plan **out, const cusmic_image *ims, si
 			throw InvalidArgument("invalid plan pointer");
 		*out = nullptr;
 		check_arguments(ims, nf, o, sc, clean, mask, false);
+		check_device_alignment(ims, nf, clean);
 		std::unique_ptr<cusmic_plan> p(new cusmic_plan);
 		check(cudaGetDevice(&p->device));
 		p->flags = flags;
@@ -847,14 +819,15 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 			check(cudaStreamSynchronize(p->last));
 		Layout L = make_layout(ims, nf, p->options, p->scalars.empty() ? nullptr : p->scalars.data(),
 			clean, mask);
-		// The plan's work lists are fixed: frames must keep their detection
-		// kernel (16-byte alignment of the bulk frames) and their sharing of
-		// error maps.
-		if (L.bulk.size() != p->L.bulk.size() || L.strips.size() != p->L.strips.size() ||
-			L.floor_base != p->L.floor_base)
-			throw InvalidArgument("rebound buffers must keep the plan's alignment and map sharing");
-		for (size_t f = 0; f < nf; ++f)
+		// The plan's threshold blocks are fixed: frames must keep their
+		// sharing of error maps.
+		check_device_alignment(ims, nf, clean);
+		if (L.thr_base != p->L.thr_base)
+			throw InvalidArgument("rebound frames must keep the plan's sharing of error maps");
+		for (size_t f = 0; f < nf; ++f) {
 			L.frames[f].bits = p->L.frames[f].bits;
+			L.frames[f].floors = p->L.frames[f].floors;
+		}
 		p->ims.assign(ims, ims + nf);
 		p->L.frames = L.frames;
 		const size_t bytes = nf * sizeof(FrameDesc);

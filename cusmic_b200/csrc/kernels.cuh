@@ -495,8 +495,13 @@ replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restric
 				lo = select_rank(fd, don, crm, win, (nd - 1) / 2);
 				hi = nd % 2 ? lo : select_rank(fd, don, crm, win, nd / 2);
 			}
-			if (lane == 0)
-				fd.clean[t.y] = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
+			if (lane == 0) {
+				const double v = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
+				fd.clean[t.y] = v;
+				// Keep the block's floor a lower bound of its clean values.
+				if (fd.floors && !fd.error)
+					atomicMin(&fd.floors[(y >> 5) * ((w + 31) >> 5) + (x >> 5)].key, order_key(v));
+			}
 			break;
 		}
 	}

@@ -343,3 +343,22 @@ def test_ragged_error_maps_mixed_alignment(cuda, oracle, mode):
         frames.append(dict(data=data, mask=mask, error=np.sqrt(np.abs(np.nan_to_num(data)) + 9),
                            background=float(10 * i)))
     check_against_oracle(oracle, frames, dict(SETTINGS, border=mode), ragged=True)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_structured_scenes_heavy_masks(cuda, oracle, seed):
+    """Piecewise sky levels (dark and bright 16 x 16 patches), dense cosmic
+    rays and a heavy mask, so replacements draw on far-away and darker donors
+    and the per-block noise floors are lowered between passes."""
+    rng = np.random.default_rng(1000 + seed)
+    h, w = int(rng.integers(40, 140)), int(rng.integers(40, 140))
+    levels = rng.choice([20.0, 300.0, 5000.0], size=((h + 15) // 16, (w + 15) // 16))
+    sky = np.kron(levels, np.ones((16, 16)))[:h, :w]
+    data = sky + rng.normal(0, 1, (h, w)) * np.sqrt(sky + 9)
+    ys, xs = rng.integers(0, h, h * w // 25), rng.integers(0, w, h * w // 25)
+    data[ys, xs] += rng.uniform(300, 20000, ys.size)
+    mask = rng.random((h, w)) < rng.uniform(0.2, 0.6)
+    mode = MODES[seed % len(MODES)]
+    frame = dict(data=data, mask=mask, gain=float(rng.uniform(1, 3)), readnoise=float(rng.uniform(2, 8)))
+    check_against_oracle(oracle, [frame], dict(SETTINGS, border=mode, gain=frame["gain"],
+                                               readnoise=frame["readnoise"]))
