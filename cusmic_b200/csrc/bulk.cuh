@@ -5,13 +5,14 @@
 // lap / (2 noise) can exceed min(cr_threshold, neighbor_threshold); the exact
 // value matters for the ~1% of pixels where it can.  So the work is split:
 //
-//  * floor_kernel (once per call, after the hole fill): a lower bound of the
-//    noise over every 32 x 32 block, turned into a threshold T = 2 min(cr, nb)
-//    (1 - 1e-12) x floor.  With an error map the floor is min(max(error, 0))
-//    over the block (NaN counts as 0), once for each distinct map.  With the
-//    noise model (src/filters.cuh:107-123) the kernel stores the smallest
-//    clean value of the block (as an ordered key) and the block's largest gain
-//    and smallest read noise.  Between passes only replacement changes clean,
+//  * block floors (once per call): a lower bound of the noise over every
+//    32 x 32 block, turned into a threshold T = 2 min(cr, nb) (1 - 1e-12) x
+//    floor.  With an error map floor_kernel takes min(max(error, 0)) over the
+//    block (NaN counts as 0), once for each distinct map.  With the noise
+//    model (src/filters.cuh:107-123) prepare_kernel stores the smallest clean
+//    value of the block (as an ordered key; holes excluded, the hole fill
+//    lowers it) and the block's largest gain and smallest read noise when
+//    they are maps.  Between passes only replacement changes clean,
 //    and replace_kernel lowers the key of the block it writes into, so the key
 //    stays a lower bound of the block's values.  Every 5 x 5 median window of
 //    a block lies in the block's 3 x 3 neighbourhood of blocks (border-mapped
@@ -85,7 +86,7 @@ constexpr int BK_CWARPS = 4;                     // consumer warps
 constexpr int BK_THREADS = 32 * (BK_CWARPS + 1); // plus one producer warp
 constexpr int BK_HALF = 64 * BK_CWARPS;          // columns of one pair set (256)
 constexpr int BK_COLS = 2 * BK_HALF;             // columns per item (512)
-constexpr int BK_ROWS = 32;                      // rows per item
+constexpr int BK_ROWS = 32;                      // most rows per item
 constexpr int BK_SLOTS = 8;                      // ring rows (power of two)
 constexpr int BK_CELLS = BK_COLS + 4;            // cells of a row: columns x0 - 2 .. x0 + BK_COLS + 1
 constexpr int BK_STRIDE = BK_CELLS + 2;          // ring row length: room for a shift of one cell
@@ -112,11 +113,10 @@ struct PreCand {
 	double lap;
 };
 
-// One 32 x 32 block whose threshold floor_kernel computes: kind FLOOR_ERROR
-// (error map; frames that share a map share its thresholds) or FLOOR_MODEL.
-enum FloorKind { FLOOR_ERROR = 0, FLOOR_MODEL = 1 };
+// One 32 x 32 block of an error map whose threshold floor_kernel computes
+// (frames that share a map share its thresholds).
 struct FloorJob {
-	int frame, x0, y0, kind;
+	int frame, x0, y0, pad;
 	long long out; // index into the threshold array
 };
 
@@ -248,8 +248,8 @@ CB_HD BulkRow bulk_row(int w, int h, int lm, int mis, int x0, int r)
 	return b;
 }
 
-// Floors of 32 x 32 blocks (see the head of this file); one warp per block,
-// one lane per column.  floors is the workspace's array; job.out indexes it.
+// Error-map floors of 32 x 32 blocks (see the head of this file), for each
+// distinct map; one warp per block, one lane per column, all 32 rows in flight.
 __global__ void __launch_bounds__(256)
 floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
 	DetectParams prm, BlockFloor *floors)
@@ -260,51 +260,26 @@ floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ 
 	for (int j = gw; j < njobs; j += nw) {
 		const FloorJob jb = jobs[j];
 		const FrameDesc &fd = frames[jb.frame];
-		const int w = fd.w, h = fd.h, x = jb.x0 + lane;
-		const int n = (jb.y0 + FLOOR_BLOCK < h ? jb.y0 + FLOOR_BLOCK : h) - jb.y0;
-		const bool in = x < w;
-		const long long at = (long long)jb.y0 * w + x;
-		if (jb.kind == FLOOR_ERROR) {
-			double m = INFINITY;
-			if (in)
-#pragma unroll 8
-				for (int k = 0; k < n; ++k) {
-					const double v = fd.error[at + (long long)k * w];
-					m = dmin(m, v > 0 ? v : 0.0);
-				}
+		const int w = fd.w, x = jb.x0 + lane;
+		const int n = (jb.y0 + FLOOR_BLOCK < fd.h ? jb.y0 + FLOOR_BLOCK : fd.h) - jb.y0;
+		const double *col = fd.error + (long long)jb.y0 * w + x;
+		double v[FLOOR_BLOCK];
 #pragma unroll
-			for (int o = 16; o; o >>= 1)
-				m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-			const double T = tmin2 * m;
-			if (lane == 0)
-				floors[jb.out].thr = T >= 0 ? T : 0.0; // NaN lists everything
-		} else {
-			unsigned long long key = ~0ull;
-			double gmax = fd.gain_map ? -INFINITY : fd.gain, rnmin = fd.rn_map ? INFINITY : fd.rn;
-			if (in)
-#pragma unroll 8
-				for (int k = 0; k < n; ++k) {
-					const long long i = at + (long long)k * w;
-					key = min(key, order_key(fd.clean[i]));
-					if (fd.gain_map)
-						gmax = dmax(gmax, fd.gain_map[i]);
-					if (fd.rn_map)
-						rnmin = dmin(rnmin, fd.rn_map[i]);
-				}
+		for (int k = 0; k < FLOOR_BLOCK; ++k)
+			v[k] = x < w && k < n ? col[(long long)k * w] : INFINITY;
+		double m = INFINITY;
 #pragma unroll
-			for (int o = 16; o; o >>= 1) {
-				key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
-				gmax = dmax(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
-				rnmin = dmin(rnmin, __shfl_xor_sync(0xffffffffu, rnmin, o));
-			}
-			if (lane == 0)
-				floors[jb.out] = BlockFloor{0.0, key, gmax, rnmin};
-		}
+		for (int k = 0; k < FLOOR_BLOCK; ++k)
+			m = dmin(m, v[k] > 0 ? v[k] : 0.0);
+#pragma unroll
+		for (int o = 16; o; o >>= 1)
+			m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+		const double T = tmin2 * m;
+		if (lane == 0)
+			floors[jb.out].thr = T >= 0 ? T : 0.0; // NaN lists everything
 	}
 }
 
-// Threshold of noise-model block (bx, by) of a bw x bh block grid from the
-// keys of its neighbourhood (see the head of this file).
 __device__ __forceinline__ int nbr_block(int b, int n, int i, bool wrap)
 {
 	// i = 0..2: b - 1 .. b + 1; i = 3..6 (wrap mode near an edge only): the two
@@ -317,9 +292,11 @@ __device__ __forceinline__ int nbr_block(int b, int n, int i, bool wrap)
 	return v >= 0 && v < n ? v : -1;
 }
 
-__device__ __forceinline__ double model_threshold(const BlockFloor *bf, int w, int h, int bx, int by,
-	int mode, double tmin2)
+__device__ __forceinline__ double model_threshold(const FrameDesc &fd, int bx, int by, int mode,
+	double tmin2)
 {
+	const BlockFloor *bf = fd.floors;
+	const int w = fd.w, h = fd.h;
 	const int bw = (w + FLOOR_BLOCK - 1) / FLOOR_BLOCK, bh = (h + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
 	const bool wrap = mode == WRAP;
 	unsigned long long key = ~0ull;
@@ -340,7 +317,9 @@ __device__ __forceinline__ double model_threshold(const BlockFloor *bf, int w, i
 	double m = order_value(key);
 	m = m < SIGNAL_FLOOR ? SIGNAL_FLOOR : m;
 	const BlockFloor &own = bf[by * bw + bx];
-	return tmin2 * (sqrt(own.rnmin * own.rnmin + own.gmax * m) / own.gmax);
+	const double g = fd.gain_map ? -order_value(own.gkey) : fd.gain;
+	const double rn = fd.rn_map ? order_value(own.rkey) : fd.rn;
+	return tmin2 * (sqrt(rn * rn + g * m) / g);
 }
 
 // Upper bound of positive(v): v when its sign bit is clear; otherwise the
@@ -404,7 +383,7 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 		const int4 it = items[t];
 		const FrameDesc &fd = frames[it.x];
 		const int w = fd.w, h = fd.h, words = fd.words, x0 = it.y, y0 = it.z;
-		const int y1 = y0 + BK_ROWS < h ? y0 + BK_ROWS : h;
+		const int y1 = it.w; // items never cross a 32-row floor block
 		const double *clean = fd.clean;
 		const int mis = (int)(((uintptr_t)clean >> 3) & 1);
 		uint32_t *s1 = plane_ptr(fd, P_S1);
@@ -504,7 +483,7 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 			if (xs[p] < w) {
 				const int bx = xs[p] / FLOOR_BLOCK;
 				double T = fd.error ? fd.floors[by * bw + bx].thr
-					: model_threshold(fd.floors, w, fd.h, bx, by, prm.mode, tmin2);
+					: model_threshold(fd, bx, by, prm.mode, tmin2);
 				ta[p] = hi_word(T >= 0 ? T : 0.0); // NaN lists everything
 			}
 			tb[p] = xs[p] + 1 < w ? ta[p] : 0xffffffffu;
@@ -732,11 +711,27 @@ classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 				if (k0 + lane < n) {
 					const PreCand pc = e[k0 + lane];
 					pix = pc.pixel;
-					const double nz = fd.error ? fd.error[pix]
-						: noise_model_at(fd, (int)(pix % (unsigned)fd.w), (int)(pix / (unsigned)fd.w),
-							prm.mode);
-					const double v = pc.lap / (2 * nz);
-					cls = v > prm.cr || v != v ? 1 : v > prm.nb ? 2 : 0;
+					if (fd.error) {
+						const double v = pc.lap / (2 * fd.error[pix]);
+						cls = v > prm.cr || v != v ? 1 : v > prm.nb ? 2 : 0;
+					} else {
+						const int px = (int)(pix % (unsigned)fd.w), py = (int)(pix / (unsigned)fd.w);
+						double nz;
+						if (px >= 2 && py >= 2 && px + 2 < fd.w && py + 2 < fd.h) {
+							double win[25];
+							const double *src = fd.clean + pix - 2 * (long long)fd.w - 2;
+#pragma unroll
+							for (int a = 0; a < 5; ++a)
+#pragma unroll
+								for (int b = 0; b < 5; ++b)
+									win[a * 5 + b] = src[(long long)a * fd.w + b];
+							nz = noise_from_median(fd, pix, median_network(win));
+						} else {
+							nz = noise_model_at(fd, px, py, prm.mode);
+						}
+						const double v = pc.lap / (2 * nz);
+						cls = v > prm.cr || v != v ? 1 : v > prm.nb ? 2 : 0;
+					}
 				}
 				const uint2 entry = make_uint2((unsigned)f, pix);
 				classify_stage(H, cls == 1, entry, &ctl->n_cand, cands, false, cap);

@@ -72,13 +72,14 @@ CB_HD int clampi(int x, int lo, int hi)
 }
 
 // Noise floor of a 32 x 32 block of a frame (see bulk.cuh): the detection
-// threshold of an error-map block, or for a noise-model block a lower bound of
-// its clean values (as an ordered key, lowered by every replacement inside
-// the block) with the block's largest gain and smallest read noise.
+// threshold of an error-map block, or for a noise-model block lower bounds
+// kept as ordered keys (a smaller key is a smaller value): of its clean values
+// (lowered by every replacement inside the block), of -gain and of the read
+// noise over the block (gain and read-noise maps only).  All-ones keys: no
+// value seen yet.
 struct BlockFloor {
 	double thr;
-	unsigned long long key;
-	double gmax, rnmin;
+	unsigned long long key, gkey, rkey;
 };
 
 // One frame of a (possibly ragged) batch, as the kernels see it.

@@ -423,12 +423,19 @@ __device__ __forceinline__ double warp_sort32(double v)
 // the seed kernel.  Only the S2 bit can be set there, and S2 is read only by
 // the second growth step, i.e. within distance 2 of a CAND pixel; candidates
 // with no CAND bit in their clipped 5 x 5 neighbourhood are skipped.
+//
+// On noise-model frames a candidate at least 4 pixels from every edge reads
+// its 25 noise windows from a 9 x 9 patch of clean staged in the warp's shared
+// memory (every position it touches is in the frame, so no border mapping is
+// needed); the others read border-mapped values from global memory.
 template <bool LOW>
 __global__ void __launch_bounds__(256)
 candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, Seed *seeds)
 {
+	__shared__ double patches[8][81];
 	const int lane = threadIdx.x & 31;
+	double *P = patches[threadIdx.x >> 5];
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)(LOW ? ctl->n_low : ctl->n_cand);
@@ -456,7 +463,28 @@ candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__
 				continue; // warp-uniform
 		}
 		double v = INFINITY, nz = 0;
-		if (lane < 25) {
+		if (!fd.error && x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+			__syncwarp();
+			const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
+			for (int k = lane; k < 81; k += 32)
+				P[k] = src[(long long)(k / 9) * w + k % 9];
+			__syncwarp();
+			if (lane < 25) {
+				const int dy = lane / 5, dx = lane % 5;
+				const double *q = P + (dy + 2) * 9 + dx + 2; // the window cell
+				const long long i = (long long)(y + dy - 2) * w + x + dx - 2;
+				{
+					double win[25];
+#pragma unroll
+					for (int a = 0; a < 5; ++a)
+#pragma unroll
+						for (int b = 0; b < 5; ++b)
+							win[a * 5 + b] = q[(a - 2) * 9 + b - 2];
+					nz = noise_from_median(fd, i, median_network(win));
+				}
+				v = lap_formula(q[0], q[-9], q[9], q[-1], q[1]) / (2 * nz);
+			}
+		} else if (lane < 25) {
 			const int mx = border_index(x + lane % 5 - 2, w, mode);
 			const int my = border_index(y + lane / 5 - 2, h, mode);
 			v = 0;
@@ -527,11 +555,18 @@ __device__ __forceinline__ double warp_rank64(double a, double b, int rank)
 
 // C: one warp per seed: 49 3 x 3 medians (two per lane), their 7 x 7 median,
 // fine structure and the contrast test (src/filters.cuh:148-175).
+//
+// A seed at least 4 pixels from every edge stages its 9 x 9 patch of clean in
+// the warp's shared memory, sorts the 63 vertical triples of the patch once,
+// and takes each 3 x 3 median from three sorted triples (median9's rule).
 __global__ void __launch_bounds__(256)
 seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds, DetectParams prm,
 	const Control *ctl)
 {
-	const int lane = threadIdx.x & 31;
+	__shared__ double patches[8][81];
+	__shared__ double triples[8][3][63]; // lo, mid, hi of rows r..r+2 of column c at r * 9 + c
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	double *P = patches[warp];
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)ctl->n_cand;
@@ -544,6 +579,34 @@ seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds
 		const int w = fd.w, h = fd.h;
 		const int x = (int)(sd.pixel % (unsigned)w), y = (int)(sd.pixel / (unsigned)w);
 		double m3[2] = {INFINITY, INFINITY};
+		if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+			__syncwarp();
+			const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
+			for (int k = lane; k < 81; k += 32)
+				P[k] = src[(long long)(k / 9) * w + k % 9];
+			__syncwarp();
+			for (int k = lane; k < 63; k += 32) {
+				double a = P[k], b = P[k + 9], c = P[k + 18];
+				cas(a, b);
+				cas(b, c);
+				cas(a, b);
+				triples[warp][0][k] = a;
+				triples[warp][1][k] = b;
+				triples[warp][2][k] = c;
+			}
+			__syncwarp();
+#pragma unroll
+			for (int s = 0; s < 2; ++s) {
+				const int j = lane + 32 * s;
+				if (j < 49) {
+					const int k = (j / 7) * 9 + j % 7; // window rows j/7 .. +2, columns j%7 .. +2
+					const double *lo = &triples[warp][0][k], *mid = &triples[warp][1][k];
+					const double *hi = &triples[warp][2][k];
+					m3[s] = med3(dmax(dmax(lo[0], lo[1]), lo[2]), med3(mid[0], mid[1], mid[2]),
+						dmin(dmin(hi[0], hi[1]), hi[2]));
+				}
+			}
+		} else {
 #pragma unroll
 		for (int s = 0; s < 2; ++s) {
 			const int j = lane + 32 * s;
@@ -563,6 +626,7 @@ seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds
 				}
 				m3[s] = m;
 			}
+		}
 		}
 		const double med3c = __shfl_sync(0xffffffffu, m3[0], 24);
 		const double med7 = warp_rank64(m3[0], m3[1], 24);

@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "backward.cuh"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -101,7 +102,7 @@ struct Layout {
 	std::vector<FrameDesc> frames;
 	std::vector<long long> bit_off; // word offset of each frame's planes
 	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, first threshold of the frame}
-	std::vector<FloorJob> jobs; // floor blocks: of each distinct error map, of each noise-model frame
+	std::vector<FloorJob> jobs; // floor blocks of each distinct error map
 	std::vector<long long> thr_base; // per frame: first floor of its blocks
 	long long nthr = 0;
 	std::vector<int2> rows;
@@ -252,9 +253,28 @@ static void check_device_alignment(const cusmic_image *ims, size_t nf, const dou
 		throw InvalidArgument("float64 buffers must be 8-byte aligned");
 }
 
-static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
-	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask)
+// Rows per item of the dense detection kernel: 32, or fewer (16, 8, 4) while
+// the batch has fewer items than the kernel has resident blocks, so small
+// frames still spread over the GPU.
+static int item_rows(const cusmic_image *ims, size_t nf, int target_items)
 {
+	int rows = BK_ROWS;
+	while (rows > 4) {
+		long long items = 0;
+		for (size_t f = 0; f < nf; ++f)
+			items += (long long)((ims[f].width + BK_COLS - 1) / BK_COLS) *
+				(long long)((ims[f].height + rows - 1) / rows);
+		if (items >= target_items)
+			break;
+		rows /= 2;
+	}
+	return rows;
+}
+
+static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
+	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask, const DeviceInfo &di)
+{
+	const int rows_per_item = item_rows(ims, nf, di.sms * BK_BLOCKS_PER_SM);
 	Layout L;
 	L.maxiter = o.maxiter;
 	L.prm.contrast = o.contrast;
@@ -307,20 +327,19 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 					base = m.second;
 		if (base < 0) {
 			base = L.nthr;
-			if (d.error)
+			if (d.error) {
 				maps[d.error].push_back({(int)f, base});
-			for (int by = 0; by < bh; ++by)
-				for (int bx = 0; bx < bw; ++bx)
-					L.jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK,
-						d.error ? FLOOR_ERROR : FLOOR_MODEL, base + (long long)by * bw + bx});
+				for (int by = 0; by < bh; ++by)
+					for (int bx = 0; bx < bw; ++bx)
+						L.jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK, 0,
+							base + (long long)by * bw + bx});
+			}
 			L.nthr += (long long)bw * bh;
 		}
-		if (base > INT_MAX)
-			throw std::bad_alloc();
 		L.thr_base[f] = base;
-		for (int ty = 0; ty < d.h; ty += BK_ROWS)
+		for (int ty = 0; ty < d.h; ty += rows_per_item)
 			for (int tx = 0; tx < d.w; tx += BK_COLS)
-				L.bulk.push_back(make_int4((int)f, tx, ty, (int)base));
+				L.bulk.push_back(make_int4((int)f, tx, ty, std::min(ty + rows_per_item, d.h)));
 	}
 	L.total_px = px;
 	L.total_words = words;
@@ -437,7 +456,8 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
 	mark(rec, K_SIGRAW);
-	classify_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
+	const int cgrid = (nbulk * BK_CWARPS + 7) / 8 < di.sms * 8 ? (nbulk * BK_CWARPS + 7) / 8 : di.sms * 8;
+	classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
 		ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
 	mark(rec, K_CLASSIFY);
 	candidate_kernel<false><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
@@ -470,13 +490,15 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		mark(rec, K_COPY);
 		return;
 	}
+	// All-ones floor keys: prepare_kernel and the fill lower them.
+	check(cudaMemsetAsync(ws.floors.p, 0xff, (size_t)L.nthr * sizeof(BlockFloor), s));
 	prepare_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
 		nrows, ws.targets.p, ws.ctl.p);
 	mark(rec, K_PREPARE);
 	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
 		&ws.ctl.p->n_holes, 1);
 	mark(rec, K_FILL);
-	// Block floors of the filled frames (replacement keeps them lower bounds).
+	// Error-map thresholds.
 	if (!L.jobs.empty()) {
 		const int nj = (int)L.jobs.size(), cap = di.sms * 8;
 		floor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p, ws.jobs.p,
@@ -571,7 +593,7 @@ static void run_device(const cusmic_image *ims, size_t nf, const cusmic_options 
 	int dev;
 	check(cudaGetDevice(&dev));
 	DeviceInfo di = device_info(dev);
-	Layout L = make_layout(ims, nf, o, sc, clean, mask);
+	Layout L = make_layout(ims, nf, o, sc, clean, mask, di);
 	Lease ws(dev);
 	upload(*ws, L, s);
 	enqueue_plain(*ws, L, di, s);
@@ -650,7 +672,7 @@ extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, d
 			gpu.mask = ws->hmask.p;
 		}
 		DeviceInfo di = device_info(dev);
-		Layout L = make_layout(&gpu, 1, *o, nullptr, ws->hclean.p, ws->hout.p);
+		Layout L = make_layout(&gpu, 1, *o, nullptr, ws->hclean.p, ws->hout.p, di);
 		upload(*ws, L, s);
 		enqueue_plain(*ws, L, di, s);
 		finish(*ws, 1, s);
@@ -792,7 +814,7 @@ extern "C" int cusmic_plan_create(cusmic_plan **out, const cusmic_image *ims, si
 		p->ims.assign(ims, ims + nf);
 		if (sc)
 			p->scalars.assign(sc, sc + nf);
-		p->L = make_layout(ims, nf, *o, sc, clean, mask);
+		p->L = make_layout(ims, nf, *o, sc, clean, mask, p->di);
 		check(cudaStreamCreateWithFlags(&p->private_stream, cudaStreamNonBlocking));
 		plan_upload(*p);
 		if (flags & CUSMIC_PLAN_GRAPH)
@@ -818,7 +840,7 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 		if (p->last)
 			check(cudaStreamSynchronize(p->last));
 		Layout L = make_layout(ims, nf, p->options, p->scalars.empty() ? nullptr : p->scalars.data(),
-			clean, mask);
+			clean, mask, p->di);
 		// The plan's threshold blocks are fixed: frames must keep their
 		// sharing of error maps.
 		check_device_alignment(ims, nf, clean);

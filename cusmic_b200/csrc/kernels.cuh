@@ -89,6 +89,28 @@ __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter
 	}
 }
 
+// IEEE bits mapped to an unsigned total order (reference src/replace.cuh:37-48).
+__device__ __forceinline__ unsigned long long order_key(double v)
+{
+	unsigned long long b = (unsigned long long)__double_as_longlong(v);
+	return (b >> 63) ? ~b : b ^ (1ull << 63);
+}
+
+__device__ __forceinline__ double order_value(unsigned long long k)
+{
+	return __longlong_as_double((long long)((k >> 63) ? k ^ (1ull << 63) : ~k));
+}
+
+// Lower *target to the warp's smallest key (one atomic per warp).
+__device__ __forceinline__ void warp_min_key(unsigned long long *target, unsigned long long k)
+{
+#pragma unroll
+	for (int o = 16; o; o >>= 1)
+		k = min(k, __shfl_xor_sync(0xffffffffu, k, o));
+	if ((threadIdx.x & 31) == 0 && k != ~0ull)
+		atomicMin(target, k);
+}
+
 // Reference src/image.cuh:24-48: holes, exclusions, clean = data (+ bg), the
 // static donor plane (the reference's is_donor with an empty mask), counts,
 // and the hole list for the initial fill (src/cleaner.cuh:78-100).  A warp
@@ -141,14 +163,26 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 					const int x = x0 + lane;
 					const bool valid = x < w;
 					bool hole = false, ok = false, donor = false;
+					double c = 0;
 					if (valid) {
 						hole = !isfinite(d[u]);
 						ok = !hole && !m[u];
-						double c = hole ? 0 : d[u];
+						c = hole ? 0 : d[u];
 						if (fd.has_bg)
 							c += 1 * bg[u];
 						fd.clean[rowpix + x] = c;
 						donor = ok && isfinite(c);
+					}
+					// Noise-model frames: block floors of clean (holes are
+					// filled later, and the fill lowers the floors itself), of
+					// -gain and of the read noise.
+					if (fd.floors && !fd.error) {
+						BlockFloor &bf = fd.floors[(y >> 5) * ((w + 31) >> 5) + (x0 >> 5)];
+						warp_min_key(&bf.key, valid && !hole ? order_key(c) : ~0ull);
+						if (fd.gain_map)
+							warp_min_key(&bf.gkey, valid ? order_key(-fd.gain_map[rowpix + x]) : ~0ull);
+						if (fd.rn_map)
+							warp_min_key(&bf.rkey, valid ? order_key(fd.rn_map[rowpix + x]) : ~0ull);
 					}
 					const uint32_t hw = __ballot_sync(0xffffffffu, hole);
 					const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
@@ -333,18 +367,6 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 		if (use_handle)
 			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
 	}
-}
-
-// IEEE bits mapped to an unsigned total order (reference src/replace.cuh:37-48).
-__device__ __forceinline__ unsigned long long order_key(double v)
-{
-	unsigned long long b = (unsigned long long)__double_as_longlong(v);
-	return (b >> 63) ? ~b : b ^ (1ull << 63);
-}
-
-__device__ __forceinline__ double order_value(unsigned long long k)
-{
-	return __longlong_as_double((long long)((k >> 63) ? k ^ (1ull << 63) : ~k));
 }
 
 // Reference src/replace.cuh:50-56.
