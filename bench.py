@@ -366,6 +366,9 @@ def ragged_comparison(dev, stream, barrier):
     plan.wait()
     px = sum(f.numel() for f in frames)
     batched = px * reps / (s.elapsed_time(e) / 1e3) / 1e6
+    prof = [plan.profile(stream) for _ in range(2)]
+    kernel_ms = {k: round(sum(p[0][k] for p in prof) / len(prof), 4)
+                 for k in _native.KERNEL_KINDS if prof[0][0][k]}
     L = _native.lib()
     msg = ctypes.create_string_buffer(256)
     ims = batch.images()
@@ -392,7 +395,7 @@ def ragged_comparison(dev, stream, barrier):
     plan.close()
     return {"frames": len(frames), "pixels": px, "batched_mpix_s": round(batched, 2),
             "plain_mpix_s": round(plain, 2), "batched_over_plain": round(batched / plain, 3),
-            "identical_masks": bool(same)}
+            "identical_masks": bool(same), "kernel_ms": kernel_ms}
 
 
 def adjoint_timing(dev, stream, barrier):

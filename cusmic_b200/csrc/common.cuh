@@ -37,6 +37,7 @@ enum Plane {
 	P_S2,     // significance > neighbor_threshold
 	P_CAND,   // seed: S1, not excluded, contrast test passed
 	P_CRMASK, // cumulative cosmic-ray mask
+	P_FRESH,  // pixels the last growth step added to the mask
 	N_PLANES
 };
 

@@ -428,9 +428,80 @@ __device__ __forceinline__ double warp_sort32(double v)
 // its 25 noise windows from a 9 x 9 patch of clean staged in the warp's shared
 // memory (every position it touches is in the frame, so no border mapping is
 // needed); the others read border-mapped values from global memory.
+// The warp's evaluation of candidate e = {frame, pixel} at (x, y); P is the
+// warp's 9 x 9 patch buffer.
 template <bool LOW>
+__device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, long long e, int x, int y,
+	double *P, const DetectParams &prm, Seed *seeds)
+{
+	const int lane = threadIdx.x & 31;
+	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
+	double v = INFINITY, nz = 0;
+	if (!fd.error && x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+		__syncwarp();
+		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
+		for (int k = lane; k < 81; k += 32)
+			P[k] = src[(long long)(k / 9) * w + k % 9];
+		__syncwarp();
+		if (lane < 25) {
+			const int dy = lane / 5, dx = lane % 5;
+			const double *q = P + (dy + 2) * 9 + dx + 2; // the window cell
+			const long long i = (long long)(y + dy - 2) * w + x + dx - 2;
+			double win[25];
+#pragma unroll
+			for (int a = 0; a < 5; ++a)
+#pragma unroll
+				for (int b = 0; b < 5; ++b)
+					win[a * 5 + b] = q[(a - 2) * 9 + b - 2];
+			nz = noise_from_median(fd, i, median_network(win));
+			v = lap_formula(q[0], q[-9], q[9], q[-1], q[1]) / (2 * nz);
+		}
+	} else if (lane < 25) {
+		const int mx = border_index(x + lane % 5 - 2, w, mode);
+		const int my = border_index(y + lane / 5 - 2, h, mode);
+		v = 0;
+		if (mx >= 0 && my >= 0) {
+			const long long i = (long long)my * w + mx;
+			nz = fd.error ? fd.error[i] : noise_model_at(fd, mx, my, mode);
+			const double lap = lap_formula(fd.clean[i], clean_at(fd, mx, my - 1, lm),
+				clean_at(fd, mx, my + 1, lm), clean_at(fd, mx - 1, my, lm),
+				clean_at(fd, mx + 1, my, lm));
+			v = lap / (2 * nz);
+		}
+	}
+	const double center = __shfl_sync(0xffffffffu, v, 12);
+	const double nz_center = __shfl_sync(0xffffffffu, nz, 12);
+	double med;
+	if (__any_sync(0xffffffffu, isnan(v))) {
+		double win[25];
+#pragma unroll
+		for (int i = 0; i < 25; ++i)
+			win[i] = __shfl_sync(0xffffffffu, v, i);
+		med = lane == 0 ? window_median_exact(win, 25) : 0.0;
+		med = __shfl_sync(0xffffffffu, med, 0);
+	} else {
+		med = __shfl_sync(0xffffffffu, warp_sort32(v), 12);
+	}
+	const double sig = center - med;
+	if (lane == 0) {
+		const long long word = (long long)y * fd.words + (x >> 5);
+		const uint32_t bit = 1u << (x & 31);
+		if (sig > prm.nb)
+			atomicOr(plane_ptr(fd, P_S2) + word, bit);
+		if (!LOW) {
+			if (sig > prm.cr)
+				atomicOr(plane_ptr(fd, P_S1) + word, bit);
+			const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
+			seeds[e] = seed ? Seed{t.x, t.y, sig, nz_center} : Seed{NO_SEED, 0, 0.0, 0.0};
+		}
+	}
+}
+
+// B, high list: one warp per candidate.  Holes have sig = 0
+// (src/filters.cuh:137-146): no bit, no seed; the dense kernel does not test
+// the hole plane itself.
 __global__ void __launch_bounds__(256)
-candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
+candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, Seed *seeds)
 {
 	__shared__ double patches[8][81];
@@ -438,90 +509,56 @@ candidate_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__
 	double *P = patches[threadIdx.x >> 5];
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-	const long long n = (long long)(LOW ? ctl->n_low : ctl->n_cand);
-	const int mode = prm.mode, lm = lap_mode(mode);
+	const long long n = (long long)ctl->n_cand;
 	for (long long e = gw; e < n; e += nw) {
-		const uint2 t = cands[LOW ? ctl->cand_cap - 1 - e : e];
+		const uint2 t = cands[e];
 		const FrameDesc &fd = frames[t.x];
-		const int w = fd.w, h = fd.h;
-		const int x = (int)(t.y % (unsigned)w), y = (int)(t.y / (unsigned)w);
-		// Holes have sig = 0 (src/filters.cuh:137-146): no bit, no seed.  The
-		// bulk dense kernel does not test the hole plane itself.
+		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
 		if (test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y)) {
-			if (!LOW && lane == 0)
+			if (lane == 0)
 				seeds[e] = Seed{NO_SEED, 0, 0.0, 0.0};
 			continue; // warp-uniform
 		}
-		if (LOW) {
-			bool near = false;
-			if (lane < 25) {
-				const int cx = x + lane % 5 - 2, cy = y + lane / 5 - 2;
-				near = cx >= 0 && cx < w && cy >= 0 && cy < h &&
-					test_bit(plane_ptr(fd, P_CAND), fd.words, cx, cy);
-			}
-			if (!__any_sync(0xffffffffu, near))
-				continue; // warp-uniform
-		}
-		double v = INFINITY, nz = 0;
-		if (!fd.error && x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
-			__syncwarp();
-			const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
-			for (int k = lane; k < 81; k += 32)
-				P[k] = src[(long long)(k / 9) * w + k % 9];
-			__syncwarp();
-			if (lane < 25) {
-				const int dy = lane / 5, dx = lane % 5;
-				const double *q = P + (dy + 2) * 9 + dx + 2; // the window cell
-				const long long i = (long long)(y + dy - 2) * w + x + dx - 2;
-				{
-					double win[25];
+		candidate_eval<false>(fd, t, e, x, y, P, prm, seeds);
+	}
+}
+
+// B, low list (run after the seed kernel): a lane per candidate first tests
+// its clipped 5 x 5 neighbourhood of the CAND plane with five 36-bit row
+// windows (S2 is read only by the second growth step, within distance 2 of a
+// CAND pixel) and its hole bit; the warp then evaluates the survivors.
+__global__ void __launch_bounds__(256)
+candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
+	DetectParams prm, Control *ctl)
+{
+	__shared__ double patches[8][81];
+	const int lane = threadIdx.x & 31;
+	double *P = patches[threadIdx.x >> 5];
+	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	const long long n = (long long)ctl->n_low;
+	const unsigned long long cap = ctl->cand_cap;
+	for (long long base = gw * 32; base < n; base += nw * 32) {
+		const long long e = base + lane;
+		uint2 t = make_uint2(0, 0);
+		bool near = false;
+		if (e < n) {
+			t = cands[cap - 1 - e];
+			const FrameDesc &fd = frames[t.x];
+			const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+			const uint32_t *cand = plane_ptr(fd, P_CAND);
+			unsigned long long any = 0;
 #pragma unroll
-					for (int a = 0; a < 5; ++a)
-#pragma unroll
-						for (int b = 0; b < 5; ++b)
-							win[a * 5 + b] = q[(a - 2) * 9 + b - 2];
-					nz = noise_from_median(fd, i, median_network(win));
-				}
-				v = lap_formula(q[0], q[-9], q[9], q[-1], q[1]) / (2 * nz);
-			}
-		} else if (lane < 25) {
-			const int mx = border_index(x + lane % 5 - 2, w, mode);
-			const int my = border_index(y + lane / 5 - 2, h, mode);
-			v = 0;
-			if (mx >= 0 && my >= 0) {
-				const long long i = (long long)my * w + mx;
-				nz = fd.error ? fd.error[i] : noise_model_at(fd, mx, my, mode);
-				const double lap = lap_formula(fd.clean[i], clean_at(fd, mx, my - 1, lm),
-					clean_at(fd, mx, my + 1, lm), clean_at(fd, mx - 1, my, lm),
-					clean_at(fd, mx + 1, my, lm));
-				v = lap / (2 * nz);
-			}
+			for (int d = -2; d <= 2; ++d)
+				any |= bit_window(cand, fd.words, fd.h, y + d, x >> 5);
+			near = ((any >> (x & 31)) & 0x1full) && !test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
 		}
-		const double center = __shfl_sync(0xffffffffu, v, 12);
-		const double nz_center = __shfl_sync(0xffffffffu, nz, 12);
-		double med;
-		if (__any_sync(0xffffffffu, isnan(v))) {
-			double win[25];
-#pragma unroll
-			for (int i = 0; i < 25; ++i)
-				win[i] = __shfl_sync(0xffffffffu, v, i);
-			med = lane == 0 ? window_median_exact(win, 25) : 0.0;
-			med = __shfl_sync(0xffffffffu, med, 0);
-		} else {
-			med = __shfl_sync(0xffffffffu, warp_sort32(v), 12);
-		}
-		const double sig = center - med;
-		if (lane == 0) {
-			const long long word = (long long)y * fd.words + (x >> 5);
-			const uint32_t bit = 1u << (x & 31);
-			if (sig > prm.nb)
-				atomicOr(plane_ptr(fd, P_S2) + word, bit);
-			if (!LOW) {
-				if (sig > prm.cr)
-					atomicOr(plane_ptr(fd, P_S1) + word, bit);
-				const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
-				seeds[e] = seed ? Seed{t.x, t.y, sig, nz_center} : Seed{NO_SEED, 0, 0.0, 0.0};
-			}
+		for (unsigned m = __ballot_sync(0xffffffffu, near); m; m &= m - 1) {
+			const int j = __ffs(m) - 1;
+			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
+			const FrameDesc &fd = frames[tj.x];
+			candidate_eval<true>(fd, tj, base + j, (int)(tj.y % (unsigned)fd.w),
+				(int)(tj.y / (unsigned)fd.w), P, prm, nullptr);
 		}
 	}
 }

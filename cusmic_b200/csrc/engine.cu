@@ -137,6 +137,7 @@ struct Workspace {
 	DevBuf<int2> rows;
 	DevBuf<uint32_t> bits;
 	DevBuf<uint2> targets;
+	DevBuf<uint8_t> radius; // per target: window radius of its last replacement
 	DevBuf<uint2> cands;
 	DevBuf<Seed> seeds;
 	DevBuf<int4> bulk;
@@ -368,6 +369,7 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	if (L.maxiter) {
 		ws.bits.ensure((size_t)L.total_words);
 		ws.targets.ensure(L.total_px);
+		ws.radius.ensure(L.total_px);
 		ws.cands.ensure(L.total_px);
 		ws.seeds.ensure(L.total_px);
 		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
@@ -460,13 +462,12 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
 		ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
 	mark(rec, K_CLASSIFY);
-	candidate_kernel<false><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
+	candidate_high_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
 		ws.seeds.p);
 	mark(rec, K_CAND);
 	seed_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p);
 	mark(rec, K_SEED);
-	candidate_kernel<true><<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
-		ws.seeds.p);
+	candidate_low_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p);
 	mark(rec, K_LOW);
 	grow_update_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.rows.p, nrows, ws.targets.p, ws.ctl.p);
@@ -474,7 +475,7 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	control_kernel<<<1, 1024, 0, s>>>(ws.state.p, nf, ws.ctl.p, gl.handle, gl.use ? 1 : 0);
 	mark(rec, K_CONTROL);
 	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
-		&ws.ctl.p->n_targets, 0);
+		&ws.ctl.p->n_targets, ws.radius.p);
 	mark(rec, K_REPLACE);
 }
 
@@ -490,13 +491,14 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		mark(rec, K_COPY);
 		return;
 	}
-	// All-ones floor keys: prepare_kernel and the fill lower them.
+	// All-ones floor keys: prepare_kernel and the fill lower them.  Zero bit
+	// planes: prepare_kernel writes HOLE, EXCL and DONOR.
 	check(cudaMemsetAsync(ws.floors.p, 0xff, (size_t)L.nthr * sizeof(BlockFloor), s));
+	check(cudaMemsetAsync(ws.bits.p, 0, (size_t)L.total_words * sizeof(uint32_t), s));
 	prepare_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
-		nrows, ws.targets.p, ws.ctl.p);
+		nrows);
 	mark(rec, K_PREPARE);
-	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
-		&ws.ctl.p->n_holes, 1);
+	fill_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows);
 	mark(rec, K_FILL);
 	// Error-map thresholds.
 	if (!L.jobs.empty()) {
@@ -1152,8 +1154,11 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 		if (!o->maxiter) {
 			copy_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
 		} else {
-			prepare_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, targets, ctl);
-			replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_holes, 1);
+			// Bit planes start at zero (prepare_kernel writes HOLE, EXCL and
+			// DONOR); the scratch keeps the previous call's contents.
+			check(cudaMemsetAsync(fd.bits, 0, (size_t)N_PLANES * L.plane * sizeof(uint32_t), s));
+			prepare_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h);
+			fill_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h);
 			for (int it = 0; it < o->maxiter; ++it) {
 				if (error_map) {
 					const int b = (L.nitems + 7) / 8 < nd.sms * 8 ? (L.nitems + 7) / 8 : nd.sms * 8;
@@ -1164,12 +1169,12 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 					sig_model_kernel<<<b, 256, 0, s>>>(frames, state, items, L.nitems, prm, ctl,
 						cands);
 				}
-				candidate_kernel<false><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
+				candidate_high_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
 				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl);
-				candidate_kernel<true><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
+				candidate_low_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl);
 				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, targets, ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
-				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, 0);
+				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, nullptr);
 			}
 			restore_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
 		}

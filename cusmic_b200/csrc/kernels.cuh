@@ -112,33 +112,35 @@ __device__ __forceinline__ void warp_min_key(unsigned long long *target, unsigne
 }
 
 // Reference src/image.cuh:24-48: holes, exclusions, clean = data (+ bg), the
-// static donor plane (the reference's is_donor with an empty mask), counts,
-// and the hole list for the initial fill (src/cleaner.cuh:78-100).  A warp
+// static donor plane (the reference's is_donor with an empty mask) and the
+// per-frame facts the initial fill needs (src/cleaner.cuh:78-100).  A warp
 // loads ROW_UNROLL chunks of 32 pixels before using them, so enough bytes are
 // in flight per SM to approach the HBM bandwidth.
 constexpr int ROW_UNROLL = 4;
 
-// Rows are taken 8 per block iteration (one per warp) with a block-uniform
-// trip count, so the block can gather its hole pixels and append them to the
-// hole list with a single atomic.
+// One warp per row (grid-stride over the row list), in segments of 32 words
+// (1024 pixels): lane j keeps the HOLE, EXCL and DONOR words of the
+// segment's word j, so each plane gets one coalesced store per segment.  The
+// other planes were zeroed before the kernel.  Holes are not listed: the hole
+// fill scans the HOLE plane.
 __global__ void __launch_bounds__(256)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
-	int nrows, uint2 *holes_out, Control *ctl)
+	int nrows)
 {
-	__shared__ int warp_holes[8];
-	__shared__ unsigned long long block_base;
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	for (int rb = blockIdx.x * 8; rb < nrows; rb += gridDim.x * 8) {
-		const int r = rb + warp;
-		int nholes = 0;
-		int2 item = make_int2(0, 0);
-		if (r < nrows) {
-			item = rows[r];
-			const FrameDesc &fd = frames[item.x];
-			const int w = fd.w, y = item.y, words = fd.words;
-			const long long rowpix = (long long)y * w, roww = (long long)y * words;
-			uint32_t any_allowed = 0, any_finite = 0;
-			for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int r = gw; r < nrows; r += nw) {
+		const int2 item = rows[r];
+		const FrameDesc &fd = frames[item.x];
+		const int w = fd.w, y = item.y, words = fd.words;
+		const long long rowpix = (long long)y * w, roww = (long long)y * words;
+		uint32_t any_hole = 0, any_allowed = 0, any_finite = 0;
+		for (int seg = 0; seg * 1024 < w; ++seg) {
+			uint32_t my_h = 0, my_e = 0, my_d = 0;
+			for (int c0 = 0; c0 < 32; c0 += ROW_UNROLL) {
+				const int xb = seg * 1024 + c0 * 32;
+				if (xb >= w)
+					break; // warp-uniform
 				double d[ROW_UNROLL], bg[ROW_UNROLL];
 				bool m[ROW_UNROLL];
 #pragma unroll
@@ -158,8 +160,6 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 #pragma unroll
 				for (int u = 0; u < ROW_UNROLL; ++u) {
 					const int x0 = xb + 32 * u;
-					if (x0 >= w)
-						break; // warp-uniform
 					const int x = x0 + lane;
 					const bool valid = x < w;
 					bool hole = false, ok = false, donor = false;
@@ -176,7 +176,7 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 					// Noise-model frames: block floors of clean (holes are
 					// filled later, and the fill lowers the floors itself), of
 					// -gain and of the read noise.
-					if (fd.floors && !fd.error) {
+					if (fd.floors && !fd.error && x0 < w) {
 						BlockFloor &bf = fd.floors[(y >> 5) * ((w + 31) >> 5) + (x0 >> 5)];
 						warp_min_key(&bf.key, valid && !hole ? order_key(c) : ~0ull);
 						if (fd.gain_map)
@@ -189,56 +189,29 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 					const uint32_t dw = __ballot_sync(0xffffffffu, donor);
 					any_allowed |= __ballot_sync(0xffffffffu, ok);
 					any_finite |= dw;
-					if (lane < N_PLANES) {
-						uint32_t v = lane == P_HOLE ? hw : lane == P_EXCL ? ew : lane == P_DONOR ? dw : 0u;
-						plane_ptr(fd, lane)[roww + (x0 >> 5)] = v;
+					any_hole |= hw;
+					if (lane == c0 + u) {
+						my_h = hw;
+						my_e = ew;
+						my_d = dw;
 					}
-					nholes += __popc(hw);
 				}
 			}
-			if (lane == 0) {
-				if (nholes)
-					set_flag(&state[item.x].holes);
-				if (any_allowed)
-					set_flag(&state[item.x].allowed);
-				if (any_finite)
-					set_flag(&state[item.x].finite);
+			const int k = seg * 32 + lane;
+			if (k < words) {
+				plane_ptr(fd, P_HOLE)[roww + k] = my_h;
+				plane_ptr(fd, P_EXCL)[roww + k] = my_e;
+				plane_ptr(fd, P_DONOR)[roww + k] = my_d;
 			}
 		}
-		if (lane == 0)
-			warp_holes[warp] = nholes;
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			int total = 0;
-			for (int i = 0; i < 8; ++i) {
-				const int c = warp_holes[i];
-				warp_holes[i] = total;
-				total += c;
-			}
-			block_base = total ? atomicAdd(&ctl->n_holes, (unsigned long long)total) : 0ull;
+		if (lane == 0) {
+			if (any_hole)
+				set_flag(&state[item.x].holes);
+			if (any_allowed)
+				set_flag(&state[item.x].allowed);
+			if (any_finite)
+				set_flag(&state[item.x].finite);
 		}
-		__syncthreads();
-		if (nholes) {
-			// Re-read this row's hole words and write its entries.
-			const FrameDesc &fd = frames[item.x];
-			const uint32_t *hp = plane_ptr(fd, P_HOLE) + (long long)item.y * fd.words;
-			unsigned long long slot = block_base + warp_holes[warp];
-			for (int k0 = 0; k0 < fd.words; k0 += 32) {
-				const int k = k0 + lane;
-				const uint32_t hw = k < fd.words ? hp[k] : 0u;
-				const unsigned long long at = slot + warp_exclusive_count(__popc(hw));
-				uint32_t bits = hw;
-				int j = 0;
-				while (bits) {
-					const int b = __ffs(bits) - 1;
-					bits &= bits - 1;
-					holes_out[at + j++] = make_uint2((unsigned)item.x,
-						(unsigned)((long long)item.y * fd.w + 32 * k + b));
-				}
-				slot += __shfl_sync(0xffffffffu, warp_inclusive_count(__popc(hw)), 31);
-			}
-		}
-		__syncthreads();
 	}
 }
 
@@ -301,6 +274,7 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 				const uint32_t now = old | grown;
 				if (fresh)
 					crm[o] = now;
+				plane_ptr(fd, P_FRESH)[o] = fresh;
 				todo |= fresh;
 				donors |= donor[o] & ~now;
 			}
@@ -465,13 +439,68 @@ __device__ double select_rank(const FrameDesc &fd, const uint32_t *don, const ui
 	return order_value(prefix);
 }
 
-// Reference src/replace.cuh:111-153 over a compacted target list, one warp per
-// target: the median of the donors in the clipped (2r+1)^2 window, r = 2, 3,
-// ... until a donor exists.  In hole mode (initial fill) a frame runs when it
-// has finite donors; otherwise when its last pass flagged new pixels.
+// Reference src/replace.cuh:111-153 for one pixel, by the whole warp: the
+// median of the donors in the clipped (2r+1)^2 window, r = 2, 3, ... until a
+// donor exists; lane 0 writes it.  Returns r (0: the frame has no donor).
+__device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y)
+{
+	const int lane = threadIdx.x & 31;
+	const int w = fd.w, h = fd.h, words = fd.words;
+	const uint32_t *don = plane_ptr(fd, P_DONOR), *crm = plane_ptr(fd, P_CRMASK);
+	const int limit = max(w, h);
+	for (int r = 2; r <= limit; ++r) {
+		Window win = {max(0, x - r), min(w - 1, x + r), max(0, y - r), min(h - 1, y + r)};
+		const int ww = win.x1 - win.x0 + 1, area = ww * (win.y1 - win.y0 + 1);
+		double lo, hi;
+		int nd;
+		if (area <= 32) {
+			bool d = false;
+			double v = INFINITY;
+			if (lane < area) {
+				int cx = win.x0 + lane % ww, cy = win.y0 + lane / ww;
+				d = donor_at(don, crm, words, cx, cy);
+				if (d)
+					v = fd.clean[(long long)cy * w + cx];
+			}
+			nd = __popc(__ballot_sync(0xffffffffu, d));
+			if (!nd)
+				continue;
+			v = bitonic32(v);
+			lo = __shfl_sync(0xffffffffu, v, (nd - 1) / 2);
+			hi = __shfl_sync(0xffffffffu, v, nd / 2);
+		} else {
+			int cnt = 0;
+			for (int pos = lane; pos < area; pos += 32)
+				cnt += donor_at(don, crm, words, win.x0 + pos % ww, win.y0 + pos / ww);
+			nd = warp_sum_int(cnt);
+			if (!nd)
+				continue;
+			lo = select_rank(fd, don, crm, win, (nd - 1) / 2);
+			hi = nd % 2 ? lo : select_rank(fd, don, crm, win, nd / 2);
+		}
+		if (lane == 0) {
+			const double v = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
+			fd.clean[(long long)y * w + x] = v;
+			// Keep the block's floor a lower bound of its clean values.
+			if (fd.floors && !fd.error)
+				atomicMin(&fd.floors[(y >> 5) * ((w + 31) >> 5) + (x >> 5)].key, order_key(v));
+		}
+		return r;
+	}
+	return 0;
+}
+
+// Replacement of the target list after a pass, one warp per target, for
+// frames whose pass flagged new pixels.
+//
+// radius (may be null) keeps, per target, the window radius of its last
+// replacement.  A target whose last window had radius 2 and in which the last
+// growth step flagged no pixel keeps its value: its donors (static donors not
+// in the mask) and their values are unchanged, so the same window and the
+// same median would come out.
 __global__ void __launch_bounds__(256)
 replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
-	const uint2 *__restrict__ list, const unsigned long long *count, int hole_mode)
+	const uint2 *__restrict__ list, const unsigned long long *count, uint8_t *radius)
 {
 	const int lane = threadIdx.x & 31;
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -479,52 +508,47 @@ replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restric
 	const long long n = (long long)*count;
 	for (long long e = gw; e < n; e += nw) {
 		const uint2 t = list[e];
-		const FrameState &st = state[t.x];
-		if (hole_mode ? !st.finite : !st.replace)
+		if (!state[t.x].replace)
 			continue;
 		const FrameDesc &fd = frames[t.x];
-		const int w = fd.w, h = fd.h, words = fd.words;
-		const int x = (int)(t.y % (unsigned)w), y = (int)(t.y / (unsigned)w);
-		const uint32_t *don = plane_ptr(fd, P_DONOR), *crm = plane_ptr(fd, P_CRMASK);
-		const int limit = max(w, h);
-		for (int r = 2; r <= limit; ++r) {
-			Window win = {max(0, x - r), min(w - 1, x + r), max(0, y - r), min(h - 1, y + r)};
-			const int ww = win.x1 - win.x0 + 1, area = ww * (win.y1 - win.y0 + 1);
-			double lo, hi;
-			int nd;
-			if (area <= 32) {
-				bool d = false;
-				double v = INFINITY;
-				if (lane < area) {
-					int cx = win.x0 + lane % ww, cy = win.y0 + lane / ww;
-					d = donor_at(don, crm, words, cx, cy);
-					if (d)
-						v = fd.clean[(long long)cy * w + cx];
-				}
-				nd = __popc(__ballot_sync(0xffffffffu, d));
-				if (!nd)
-					continue;
-				v = bitonic32(v);
-				lo = __shfl_sync(0xffffffffu, v, (nd - 1) / 2);
-				hi = __shfl_sync(0xffffffffu, v, nd / 2);
-			} else {
-				int cnt = 0;
-				for (int pos = lane; pos < area; pos += 32)
-					cnt += donor_at(don, crm, words, win.x0 + pos % ww, win.y0 + pos / ww);
-				nd = warp_sum_int(cnt);
-				if (!nd)
-					continue;
-				lo = select_rank(fd, don, crm, win, (nd - 1) / 2);
-				hi = nd % 2 ? lo : select_rank(fd, don, crm, win, nd / 2);
+		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+		if (radius && radius[e] == 2) {
+			const uint32_t *fr = plane_ptr(fd, P_FRESH);
+			unsigned long long any = 0;
+#pragma unroll
+			for (int d = -2; d <= 2; ++d)
+				any |= bit_window(fr, fd.words, fd.h, y + d, x >> 5);
+			if (!((any >> (x & 31)) & 0x1full))
+				continue; // warp-uniform
+		}
+		const int r = replace_one(fd, x, y);
+		if (radius && lane == 0)
+			radius[e] = (uint8_t)(r < 255 ? r : 255);
+	}
+}
+
+// Initial fill of non-finite pixels (src/cleaner.cuh:78-100) for frames with
+// a finite donor: one warp per row scans the row's HOLE words.
+__global__ void __launch_bounds__(256)
+fill_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
+	const int2 *__restrict__ rows, int nrows)
+{
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int ri = gw; ri < nrows; ri += nw) {
+		const int2 item = rows[ri];
+		const FrameState &st = state[item.x];
+		if (!st.holes || !st.finite)
+			continue; // warp-uniform
+		const FrameDesc &fd = frames[item.x];
+		const uint32_t *hp = plane_ptr(fd, P_HOLE) + (long long)item.y * fd.words;
+		for (int k0 = 0; k0 < fd.words; k0 += 32) {
+			const uint32_t hw = k0 + lane < fd.words ? hp[k0 + lane] : 0u;
+			for (unsigned m = __ballot_sync(0xffffffffu, hw != 0); m; m &= m - 1) {
+				const int j = __ffs(m) - 1;
+				for (uint32_t bits = __shfl_sync(0xffffffffu, hw, j); bits; bits &= bits - 1)
+					replace_one(fd, 32 * (k0 + j) + __ffs(bits) - 1, item.y);
 			}
-			if (lane == 0) {
-				const double v = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
-				fd.clean[t.y] = v;
-				// Keep the block's floor a lower bound of its clean values.
-				if (fd.floors && !fd.error)
-					atomicMin(&fd.floors[(y >> 5) * ((w + 31) >> 5) + (x >> 5)].key, order_key(v));
-			}
-			break;
 		}
 	}
 }
