@@ -563,10 +563,16 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 	for (int r = gw; r < nrows; r += nw) {
 		const int2 item = rows[r];
 		const FrameDesc &fd = frames[item.x];
+		// Descriptor fields in registers (the stores below could alias it).
 		const int w = fd.w, y = item.y, words = fd.words;
 		const uint32_t *hole = plane_ptr(fd, P_HOLE) + (long long)y * words;
 		const uint32_t *crm = plane_ptr(fd, P_CRMASK) + (long long)y * words;
 		const long long rowpix = (long long)y * w;
+		double *clean = fd.clean + rowpix;
+		const double *data = fd.data + rowpix, *bgmap = fd.bg_map ? fd.bg_map + rowpix : nullptr;
+		uint8_t *mask_out = fd.mask_out + rowpix;
+		const double bgv = fd.bg;
+		const bool has_bg = fd.has_bg;
 		for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
 			double v[ROW_UNROLL], bg[ROW_UNROLL];
 			uint32_t hb[ROW_UNROLL], cb[ROW_UNROLL];
@@ -574,14 +580,14 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 			for (int u = 0; u < ROW_UNROLL; ++u) {
 				const int x = xb + 32 * u + lane;
 				v[u] = 0;
-				bg[u] = fd.bg;
+				bg[u] = bgv;
 				hb[u] = cb[u] = 0;
 				if (x < w) {
-					v[u] = fd.clean[rowpix + x];
+					v[u] = clean[x];
 					hb[u] = hole[x >> 5];
 					cb[u] = crm[x >> 5];
-					if (fd.bg_map)
-						bg[u] = fd.bg_map[rowpix + x];
+					if (bgmap)
+						bg[u] = bgmap[x];
 				}
 			}
 #pragma unroll
@@ -589,12 +595,12 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 				const int x = xb + 32 * u + lane;
 				if (x < w) {
 					double o = v[u];
-					if (fd.has_bg)
+					if (has_bg)
 						o += -1 * bg[u];
 					if ((hb[u] >> (x & 31)) & 1u)
-						o = fd.data[rowpix + x];
-					fd.clean[rowpix + x] = o;
-					fd.mask_out[rowpix + x] = (cb[u] >> (x & 31)) & 1u;
+						o = data[x];
+					clean[x] = o;
+					mask_out[x] = (cb[u] >> (x & 31)) & 1u;
 				}
 			}
 		}
