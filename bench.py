@@ -58,6 +58,7 @@ def parse_args():
     p.add_argument("--frames", type=int, default=16)
     p.add_argument("--size", type=int, default=2048)
     p.add_argument("--no-extras", action="store_true", help="skip plain/ragged comparisons")
+    p.add_argument("--no-large", action="store_true", help="skip the 4 x 8192^2 forward/backward run")
     p.add_argument("--cpu-sample-rows", type=int, default=1024,
                    help="rows of one frame timed for the CPU baseline")
     return p.parse_args()
@@ -298,6 +299,8 @@ def main():
         out["plain"] = plain_vs_batched(plan, batch, stream, value / world, barrier)
         out["ragged"] = ragged_comparison(dev, stream, barrier)
         out["adjoint"] = adjoint_timing(dev, stream, barrier)
+        if not args.no_large:
+            out["large"] = large_run(dev, stream, barrier)
 
     if rank == 0:
         v, dt, n = cpu_reference(sc.frames[0].data, sc.error, sc.mask, args.cpu_sample_rows)
@@ -396,6 +399,59 @@ def ragged_comparison(dev, stream, barrier):
     return {"frames": len(frames), "pixels": px, "batched_mpix_s": round(batched, 2),
             "plain_mpix_s": round(plain, 2), "batched_over_plain": round(batched / plain, 3),
             "identical_masks": bool(same), "kernel_ms": kernel_ms}
+
+
+def large_run(dev, stream, barrier):
+    """large_8192: forward and frozen-mask backward of 4 x 8192^2 float64 frames
+    (full-size error map, 2% mask), with the device memory the process holds."""
+    import torch
+    from cusmic_b200 import scenes
+    from cusmic_b200.plan import Plan, Batch
+    free0, total = torch.cuda.mem_get_info(dev)
+    sc = scenes.large_8192(seed=0)
+    stack = torch.from_numpy(np.stack([f.data for f in sc.frames])).to(dev)
+    del sc.frames[:]
+    batch = Batch.stack(stack, error=torch.from_numpy(sc.error).to(dev),
+                        mask=torch.from_numpy(sc.mask.astype(np.uint8)).to(dev))
+    plan = Plan(batch, graph=True, keep=True, **SETTINGS)
+    g = torch.randn(stack.shape, dtype=torch.float64, device=dev,
+                    generator=torch.Generator(device=dev).manual_seed(0))
+    plan.execute(stream)
+    plan.wait()
+    first_mask = batch.mask_out.clone()
+    plan.backward(g, stream)
+    torch.cuda.synchronize(dev)
+    reps = 3
+    fwd = bwd = 0.0
+    for _ in range(reps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        s.record(stream)
+        plan.execute(stream)
+        e.record(stream)
+        plan.wait()
+        fwd += s.elapsed_time(e)
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s2.record(stream)
+        gx, _ = plan.backward(g, stream)
+        e2.record(stream)
+        torch.cuda.synchronize(dev)
+        bwd += s2.elapsed_time(e2)
+        del gx
+    free1, _ = torch.cuda.mem_get_info(dev)
+    px = stack.numel()
+    out = {"workload": "large_8192: 4 x 8192x8192 float64, full error map, 2% mask, 3000 rays "
+                       "(10% tracks 10-40 px), 200 saturated stars, forward + frozen-mask backward",
+           "fwd_ms": round(fwd / reps, 3), "bwd_ms": round(bwd / reps, 3),
+           "bwd_over_fwd": round(bwd / fwd, 4), "fwd_mpix_s": round(px * reps / (fwd / 1e3) / 1e6, 1),
+           "flagged": int(batch.mask_out.sum()),
+           "repeatable": bool(torch.equal(first_mask, batch.mask_out)),
+           "device_gb_held": round((total - free1) / 1e9, 2),
+           "device_gb_before": round((total - free0) / 1e9, 2)}
+    plan.close()
+    del batch, stack, g
+    torch.cuda.empty_cache()
+    return out
 
 
 def adjoint_timing(dev, stream, barrier):
