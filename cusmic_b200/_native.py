@@ -6,6 +6,7 @@ importing the Python API without it raises immediately.
 """
 
 import ctypes
+import json
 from pathlib import Path
 
 LIB_PATH = Path(__file__).with_name("libcusmic_b200.so")
@@ -20,8 +21,9 @@ EXPORTS = (
     "remove_cosmics_device", "remove_cosmics_batch_device", "cusmic_ragged_batch_device",
     "cusmic_plan_create", "cusmic_plan_bind", "cusmic_plan_execute", "cusmic_plan_wait",
     "cusmic_plan_passes", "cusmic_plan_profile", "cusmic_plan_backward", "cusmic_plan_destroy",
-    "remove_cosmics_device_noalloc",
+    "remove_cosmics_device_noalloc", "cusmic_set_tuning", "cusmic_get_tuning",
 )
+TUNING_PATH = Path(__file__).with_name("tuning.json")
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
                 "replace", "restore", "copy", "low", "classify", "floor")
 
@@ -45,6 +47,19 @@ class FrameScalars(ctypes.Structure):
     """struct cusmic_frame_scalars."""
     _fields_ = [("gain", ctypes.c_double), ("readnoise", ctypes.c_double),
                 ("background", ctypes.c_double)]
+
+
+class Tuning(ctypes.Structure):
+    """struct cusmic_tuning."""
+    _fields_ = [("max_pixels", ctypes.c_size_t), ("dense_rows", ctypes.c_int),
+                ("dense_blocks_per_sm", ctypes.c_int), ("sparse_blocks_per_sm", ctypes.c_int),
+                ("row_blocks_per_sm", ctypes.c_int)]
+
+    FIELDS = ("max_pixels", "dense_rows", "dense_blocks_per_sm", "sparse_blocks_per_sm",
+              "row_blocks_per_sm")
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k in self.FIELDS}
 
 
 class CusmicError(RuntimeError):
@@ -97,8 +112,33 @@ def lib():
     L.cusmic_plan_destroy.argtypes = [vp]
     L.remove_cosmics_device_noalloc.restype = ip
     L.remove_cosmics_device_noalloc.argtypes = [img, opt, vp, vp, vp, cp, sz]
+    L.cusmic_set_tuning.restype = ip
+    L.cusmic_set_tuning.argtypes = [ctypes.POINTER(Tuning), sz, cp, sz]
+    L.cusmic_get_tuning.restype = ip
+    L.cusmic_get_tuning.argtypes = [sz, ctypes.POINTER(Tuning)]
     _lib = L
+    if TUNING_PATH.exists():
+        set_tuning(json.loads(TUNING_PATH.read_text())["table"])
     return L
+
+
+def set_tuning(entries):
+    """Install a tuning table: a list of dicts with Tuning's fields (max_pixels
+    may be null for "no limit"); an empty list restores the built-in defaults."""
+    arr = (Tuning * max(1, len(entries)))()
+    for i, e in enumerate(entries):
+        mp = e.get("max_pixels")
+        arr[i] = Tuning(2 ** 64 - 1 if mp is None else int(mp), int(e["dense_rows"]),
+                        int(e["dense_blocks_per_sm"]), int(e["sparse_blocks_per_sm"]),
+                        int(e["row_blocks_per_sm"]))
+    msg = ctypes.create_string_buffer(256)
+    raise_for(lib().cusmic_set_tuning(arr, len(entries), msg, 256), msg)
+
+
+def get_tuning(total_pixels):
+    t = Tuning()
+    raise_for(lib().cusmic_get_tuning(int(total_pixels), ctypes.byref(t)), "invalid tuning query")
+    return t.as_dict()
 
 
 def default_options():

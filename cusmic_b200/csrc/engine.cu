@@ -97,6 +97,24 @@ template <class T> struct PinBuf {
 	}
 };
 
+// Launch parameters (include/cusmic_b200.h, struct cusmic_tuning).
+static std::mutex tuning_mu;
+static std::vector<cusmic_tuning> tuning_table;
+
+static cusmic_tuning default_tuning(size_t)
+{
+	return cusmic_tuning{SIZE_MAX, 0, BK_BLOCKS_PER_SM, 8, 8};
+}
+
+static cusmic_tuning tuning_for(size_t total_px)
+{
+	std::lock_guard<std::mutex> lock(tuning_mu);
+	for (const cusmic_tuning &t : tuning_table)
+		if (total_px <= t.max_pixels)
+			return t;
+	return default_tuning(total_px);
+}
+
 // Host description of one batch.
 struct Layout {
 	std::vector<FrameDesc> frames;
@@ -111,6 +129,7 @@ struct Layout {
 	size_t total_px = 0;
 	DetectParams prm{};
 	int maxiter = 0;
+	cusmic_tuning tune{};
 };
 
 struct DeviceInfo {
@@ -275,8 +294,14 @@ static int item_rows(const cusmic_image *ims, size_t nf, int target_items)
 static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
 	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask, const DeviceInfo &di)
 {
-	const int rows_per_item = item_rows(ims, nf, di.sms * BK_BLOCKS_PER_SM);
+	size_t all_px = 0;
+	for (size_t f = 0; f < nf; ++f)
+		all_px += ims[f].width * ims[f].height;
+	const cusmic_tuning tune = tuning_for(all_px);
+	const int rows_per_item = tune.dense_rows ? tune.dense_rows
+		: item_rows(ims, nf, di.sms * tune.dense_blocks_per_sm);
 	Layout L;
+	L.tune = tune;
 	L.maxiter = o.maxiter;
 	L.prm.contrast = o.contrast;
 	L.prm.cr = o.cr_threshold;
@@ -347,10 +372,10 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 	return L;
 }
 
-static int grid_for_rows(const DeviceInfo &di, size_t nrows)
+static int grid_for_rows(const DeviceInfo &di, size_t nrows, int blocks_per_sm = 8)
 {
 	size_t blocks = (nrows + 7) / 8;
-	size_t cap = (size_t)di.sms * 8;
+	size_t cap = (size_t)di.sms * blocks_per_sm;
 	return (int)(blocks < 1 ? 1 : blocks > cap ? cap : blocks);
 }
 
@@ -454,27 +479,28 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
 	const int nbulk = (int)L.bulk.size();
-	const int cap = di.sms * BK_BLOCKS_PER_SM;
+	const int cap = di.sms * L.tune.dense_blocks_per_sm, sparse = di.sms * L.tune.sparse_blocks_per_sm;
+	const int rowb = L.tune.row_blocks_per_sm;
 	sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
 	mark(rec, K_SIGRAW);
-	const int cgrid = (nbulk * BK_CWARPS + 7) / 8 < di.sms * 8 ? (nbulk * BK_CWARPS + 7) / 8 : di.sms * 8;
+	const int cgrid = (nbulk * BK_CWARPS + 7) / 8 < sparse ? (nbulk * BK_CWARPS + 7) / 8 : sparse;
 	classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
 		ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
 	mark(rec, K_CLASSIFY);
-	candidate_high_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
+	candidate_high_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
 		ws.seeds.p);
 	mark(rec, K_CAND);
-	seed_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p);
+	seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p);
 	mark(rec, K_SEED);
-	candidate_low_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p);
+	candidate_low_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p);
 	mark(rec, K_LOW);
-	grow_update_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p,
+	grow_update_kernel<<<grid_for_rows(di, nrows, rowb), 256, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.rows.p, nrows, ws.targets.p, ws.ctl.p);
 	mark(rec, K_GROW);
 	control_kernel<<<1, 1024, 0, s>>>(ws.state.p, nf, ws.ctl.p, gl.handle, gl.use ? 1 : 0);
 	mark(rec, K_CONTROL);
-	replace_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
+	replace_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
 		&ws.ctl.p->n_targets, ws.radius.p);
 	mark(rec, K_REPLACE);
 }
@@ -495,10 +521,10 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	// planes: prepare_kernel writes HOLE, EXCL and DONOR.
 	check(cudaMemsetAsync(ws.floors.p, 0xff, (size_t)L.nthr * sizeof(BlockFloor), s));
 	check(cudaMemsetAsync(ws.bits.p, 0, (size_t)L.total_words * sizeof(uint32_t), s));
-	prepare_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
+	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
 		nrows);
 	mark(rec, K_PREPARE);
-	fill_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows);
+	fill_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows);
 	mark(rec, K_FILL);
 	// Error-map thresholds.
 	if (!L.jobs.empty()) {
@@ -515,7 +541,7 @@ static void launch_epilogue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	if (!L.maxiter)
 		return;
 	const int nrows = (int)L.rows.size();
-	restore_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
+	restore_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
 	mark(rec, K_RESTORE);
 }
 
@@ -1089,6 +1115,33 @@ static NoallocDevice noalloc_device(int dev)
 }
 
 } // namespace cb
+
+extern "C" int cusmic_set_tuning(const cusmic_tuning *table, size_t n, char *msg, size_t len)
+{
+	return guarded([&] {
+		if (n && !table)
+			throw InvalidArgument("invalid tuning table");
+		for (size_t i = 0; i < n; ++i) {
+			const cusmic_tuning &t = table[i];
+			if (!(t.dense_rows == 0 || t.dense_rows == 4 || t.dense_rows == 8 || t.dense_rows == 16 ||
+				    t.dense_rows == 32) ||
+				t.dense_blocks_per_sm < 1 || t.dense_blocks_per_sm > BK_BLOCKS_PER_SM ||
+				t.sparse_blocks_per_sm < 1 || t.sparse_blocks_per_sm > 8 ||
+				t.row_blocks_per_sm < 1 || t.row_blocks_per_sm > 8)
+				throw InvalidArgument("invalid tuning entry");
+		}
+		std::lock_guard<std::mutex> lock(tuning_mu);
+		tuning_table.assign(table, table + n);
+	}, msg, len);
+}
+
+extern "C" int cusmic_get_tuning(size_t total_pixels, cusmic_tuning *out)
+{
+	if (!out)
+		return CUSMIC_INVALID;
+	*out = tuning_for(total_pixels);
+	return CUSMIC_OK;
+}
 
 extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmic_options *o,
 	double *clean, uint8_t *mask, void *stream, char *msg, size_t len)

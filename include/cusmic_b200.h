@@ -108,6 +108,34 @@ cusmic_plan_backward(cusmic_plan *plan, const double *grad_clean, double *grad_d
 void
 cusmic_plan_destroy(cusmic_plan *plan);
 
+/* Launch parameters of the detection pass, chosen per batch size by the
+ * project's autotuner (cusmic_b200/autotune.py; results in
+ * cusmic_b200/tuning.json).  An entry applies to batches of at most
+ * max_pixels pixels; the first matching entry of the table wins. */
+struct cusmic_tuning {
+	size_t max_pixels;
+	int dense_rows;           /* rows per item of the dense detection kernel: 4, 8, 16
+	                             or 32; 0 = automatic (shrink from 32 while the batch
+	                             has fewer items than the kernel has resident blocks) */
+	int dense_blocks_per_sm;  /* dense detection blocks launched per SM: 1..6 */
+	int sparse_blocks_per_sm; /* 256-thread blocks per SM of the candidate, seed,
+	                             low-candidate, classification and replacement
+	                             kernels: 1..8 */
+	int row_blocks_per_sm;    /* 256-thread blocks per SM of the row kernels (prepare,
+	                             hole fill, growth, restore): 1..8 */
+};
+
+/* Replace the process-wide tuning table (n entries, copied; n = 0 restores the
+ * built-in defaults).  Plans keep the parameters they were created with.
+ * CUSMIC_INVALID for out-of-range fields.  No counterpart in the reference. */
+int
+cusmic_set_tuning(const struct cusmic_tuning *table, size_t n, char *msg, size_t message_size);
+
+/* The entry that applies to a batch of total_pixels pixels.  No counterpart in
+ * the reference. */
+int
+cusmic_get_tuning(size_t total_pixels, struct cusmic_tuning *out);
+
 /* remove_cosmics_device for callers that cannot allocate device memory when
  * they clean a frame: code being captured into a CUDA graph (cudaMalloc and
  * cudaFree are not stream-ordered; cudaFree synchronises the device), real-time

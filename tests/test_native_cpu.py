@@ -124,3 +124,27 @@ def test_cleaner_settings():
                      {"border_mode": "invalid"}):
         with pytest.raises(ValueError):
             Cleaner(**settings)
+
+
+def test_tuning_table_validation_and_lookup():
+    from cusmic_b200 import _native
+    saved = [_native.get_tuning(0)]
+    try:
+        _native.set_tuning([dict(max_pixels=1000, dense_rows=8, dense_blocks_per_sm=4,
+                                 sparse_blocks_per_sm=2, row_blocks_per_sm=6),
+                            dict(max_pixels=None, dense_rows=0, dense_blocks_per_sm=6,
+                                 sparse_blocks_per_sm=8, row_blocks_per_sm=8)])
+        assert _native.get_tuning(999)["dense_rows"] == 8
+        assert _native.get_tuning(1000)["row_blocks_per_sm"] == 6
+        assert _native.get_tuning(1001)["dense_blocks_per_sm"] == 6
+        for bad in (dict(dense_rows=3), dict(dense_blocks_per_sm=0), dict(dense_blocks_per_sm=7),
+                    dict(sparse_blocks_per_sm=9), dict(row_blocks_per_sm=0)):
+            entry = dict(dict(max_pixels=None, dense_rows=0, dense_blocks_per_sm=6,
+                              sparse_blocks_per_sm=8, row_blocks_per_sm=8), **bad)
+            with pytest.raises(ValueError, match="invalid tuning entry"):
+                _native.set_tuning([entry])
+        _native.set_tuning([])
+        d = _native.get_tuning(12345)
+        assert (d["dense_rows"], d["dense_blocks_per_sm"]) == (0, 6)
+    finally:
+        _native.set_tuning(saved)
