@@ -47,6 +47,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Mpix/s (f64, maxiter=4, identical masks) batched vs plain; bwd/fwd time"
 SETTINGS = dict(contrast=3.0, cr_threshold=5.0, neighbor_threshold=3.0, maxiter=4)
+SIG_BULK_DRAM_BYTES_PER_PX = 8.86  # ncu: 148.7 MB per launch over 16.78 Mpix
 
 
 def parse_args():
@@ -228,21 +229,25 @@ def main():
     kinds = _native.KERNEL_KINDS
     kms = {k: sum(p[0][k] for p in prof) / len(prof) for k in kinds}
     klaunch = {k: prof[0][1][k] for k in kinds}
-    # Dense detection kernel (sig_bulk_kernel: the stack's rows are 16-byte
-    # aligned): per pixel of an active frame it must read clean (8 B) and clear
-    # the S1/S2/CAND bits (3/8 B); the shared error map (8 B/px) counts once
-    # per launch.
+    # Dense detection kernel (sig_bulk_kernel): per pixel of an active frame it
+    # must read clean (8 B) and clear the S1/S2/CAND bits (3/8 B).  The error
+    # map is not read there: its 32 x 32 block floors are computed once per
+    # call by floor_kernel.
     active_px = sum(passes) * h * w
-    detect_bytes = active_px * (8 + 3 / 8) + klaunch["sigraw"] * h * w * 8
+    detect_bytes = active_px * (8 + 3 / 8)
     detect_ms = kms["sigraw"]
     achieved = detect_bytes / (detect_ms / 1e3) / 1e9
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
         if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     total_kernel_ms = sum(kms.values())
+    # DRAM bytes per active pixel of one sig_bulk_kernel launch from an ncu
+    # capture (profiles/sig_bulk_kernel_stack_2048_4frames.md), scaled to this
+    # launch's active pixels.
+    traffic = active_px * SIG_BULK_DRAM_BYTES_PER_PX / max(1, klaunch["sigraw"])
     roofline = {"bound": "hbm", "kernel": "sig_bulk_kernel", "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": None, "peak_source": "measured" if peaks else "fallback",
+                "traffic": round(traffic), "peak_source": "measured" if peaks else "fallback",
                 "algorithmic_bytes_per_launch": round(detect_bytes / max(1, klaunch["sigraw"])),
                 "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4),
                 "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
