@@ -428,11 +428,12 @@ __device__ __forceinline__ double warp_sort32(double v)
 // its 25 noise windows from a 9 x 9 patch of clean staged in the warp's shared
 // memory (every position it touches is in the frame, so no border mapping is
 // needed); the others read border-mapped values from global memory.
-// The warp's evaluation of candidate e = {frame, pixel} at (x, y); P is the
-// warp's 9 x 9 patch buffer.
+// The warp's evaluation of the candidate at (x, y): sig over its 5 x 5
+// window, the S2 bit (and S1 unless LOW); returns sig (every lane) and the
+// noise at the pixel (nz_center).  P is the warp's 9 x 9 patch buffer.
 template <bool LOW>
-__device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, long long e, int x, int y,
-	double *P, const DetectParams &prm, Seed *seeds)
+__device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int y, double *P,
+	const DetectParams &prm, double &nz_center_out)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
@@ -488,12 +489,24 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 		const uint32_t bit = 1u << (x & 31);
 		if (sig > prm.nb)
 			atomicOr(plane_ptr(fd, P_S2) + word, bit);
-		if (!LOW) {
-			if (sig > prm.cr)
-				atomicOr(plane_ptr(fd, P_S1) + word, bit);
-			const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
-			seeds[e] = seed ? Seed{t.x, t.y, sig, nz_center} : Seed{NO_SEED, 0, 0.0, 0.0};
-		}
+		if (!LOW && sig > prm.cr)
+			atomicOr(plane_ptr(fd, P_S1) + word, bit);
+	}
+	nz_center_out = nz_center;
+	return sig;
+}
+
+// candidate_sig plus the seed slot of candidate e (list-based kernels).
+template <bool LOW>
+__device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, long long e, int x, int y,
+	double *P, const DetectParams &prm, Seed *seeds)
+{
+	double nz;
+	const double sig = candidate_sig<LOW>(fd, x, y, P, prm, nz);
+	if (!LOW && (threadIdx.x & 31) == 0) {
+		const long long word = (long long)y * fd.words + (x >> 5);
+		const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & (1u << (x & 31)));
+		seeds[e] = seed ? Seed{t.x, t.y, sig, nz} : Seed{NO_SEED, 0, 0.0, 0.0};
 	}
 }
 
@@ -590,60 +603,45 @@ __device__ __forceinline__ double warp_rank64(double a, double b, int rank)
 	return rank < 32 ? ra : rb;
 }
 
-// C: one warp per seed: 49 3 x 3 medians (two per lane), their 7 x 7 median,
-// fine structure and the contrast test (src/filters.cuh:148-175).
-//
-// A seed at least 4 pixels from every edge stages its 9 x 9 patch of clean in
-// the warp's shared memory, sorts the 63 vertical triples of the patch once,
-// and takes each 3 x 3 median from three sorted triples (median9's rule).
-__global__ void __launch_bounds__(256)
-seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds, DetectParams prm,
-	const Control *ctl)
+// The warp's fine-structure test of a seed at (x, y) (src/filters.cuh:148-175):
+// 49 3 x 3 medians (two per lane), their 7 x 7 median, fine structure and the
+// contrast test, setting the CAND bit.  A seed at least 4 pixels from every
+// edge stages its 9 x 9 patch of clean in the warp's shared memory (P), sorts
+// the 63 vertical triples of the patch once (T) and takes each 3 x 3 median
+// from three sorted triples (median9's rule).
+__device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, double sig, double noise,
+	const DetectParams &prm, double *P, double (*T)[63])
 {
-	__shared__ double patches[8][81];
-	__shared__ double triples[8][3][63]; // lo, mid, hi of rows r..r+2 of column c at r * 9 + c
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	double *P = patches[warp];
-	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-	const long long n = (long long)ctl->n_cand;
-	const int mode = prm.mode;
-	for (long long e = gw; e < n; e += nw) {
-		const Seed sd = seeds[e];
-		if (sd.frame == NO_SEED)
-			continue; // warp-uniform
-		const FrameDesc &fd = frames[sd.frame];
-		const int w = fd.w, h = fd.h;
-		const int x = (int)(sd.pixel % (unsigned)w), y = (int)(sd.pixel / (unsigned)w);
-		double m3[2] = {INFINITY, INFINITY};
-		if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
-			__syncwarp();
-			const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
-			for (int k = lane; k < 81; k += 32)
-				P[k] = src[(long long)(k / 9) * w + k % 9];
-			__syncwarp();
-			for (int k = lane; k < 63; k += 32) {
-				double a = P[k], b = P[k + 9], c = P[k + 18];
-				cas(a, b);
-				cas(b, c);
-				cas(a, b);
-				triples[warp][0][k] = a;
-				triples[warp][1][k] = b;
-				triples[warp][2][k] = c;
-			}
-			__syncwarp();
+	const int lane = threadIdx.x & 31;
+	const int w = fd.w, h = fd.h, mode = prm.mode;
+	double m3[2] = {INFINITY, INFINITY};
+	if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+		__syncwarp();
+		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
+		for (int k = lane; k < 81; k += 32)
+			P[k] = src[(long long)(k / 9) * w + k % 9];
+		__syncwarp();
+		for (int k = lane; k < 63; k += 32) {
+			double a = P[k], b = P[k + 9], c = P[k + 18];
+			cas(a, b);
+			cas(b, c);
+			cas(a, b);
+			T[0][k] = a;
+			T[1][k] = b;
+			T[2][k] = c;
+		}
+		__syncwarp();
 #pragma unroll
-			for (int s = 0; s < 2; ++s) {
-				const int j = lane + 32 * s;
-				if (j < 49) {
-					const int k = (j / 7) * 9 + j % 7; // window rows j/7 .. +2, columns j%7 .. +2
-					const double *lo = &triples[warp][0][k], *mid = &triples[warp][1][k];
-					const double *hi = &triples[warp][2][k];
-					m3[s] = med3(dmax(dmax(lo[0], lo[1]), lo[2]), med3(mid[0], mid[1], mid[2]),
-						dmin(dmin(hi[0], hi[1]), hi[2]));
-				}
+		for (int s = 0; s < 2; ++s) {
+			const int j = lane + 32 * s;
+			if (j < 49) {
+				const int k = (j / 7) * 9 + j % 7; // window rows j/7 .. +2, columns j%7 .. +2
+				const double *lo = &T[0][k], *mid = &T[1][k], *hi = &T[2][k];
+				m3[s] = med3(dmax(dmax(lo[0], lo[1]), lo[2]), med3(mid[0], mid[1], mid[2]),
+					dmin(dmin(hi[0], hi[1]), hi[2]));
 			}
-		} else {
+		}
+	} else {
 #pragma unroll
 		for (int s = 0; s < 2; ++s) {
 			const int j = lane + 32 * s;
@@ -664,15 +662,35 @@ seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds
 				m3[s] = m;
 			}
 		}
-		}
-		const double med3c = __shfl_sync(0xffffffffu, m3[0], 24);
-		const double med7 = warp_rank64(m3[0], m3[1], 24);
-		if (lane == 0) {
-			double fine = (med3c - med7) / sd.noise;
-			fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
-			if (sd.sig / fine > prm.contrast)
-				atomicOr(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
-		}
+	}
+	const double med3c = __shfl_sync(0xffffffffu, m3[0], 24);
+	const double med7 = warp_rank64(m3[0], m3[1], 24);
+	if (lane == 0) {
+		double fine = (med3c - med7) / noise;
+		fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
+		if (sig / fine > prm.contrast)
+			atomicOr(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
+	}
+}
+
+// C (list-based): one warp per seed slot.
+__global__ void __launch_bounds__(256)
+seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds, DetectParams prm,
+	const Control *ctl)
+{
+	__shared__ double patches[8][81];
+	__shared__ double triples[8][3][63];
+	const int warp = threadIdx.x >> 5;
+	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	const long long n = (long long)ctl->n_cand;
+	for (long long e = gw; e < n; e += nw) {
+		const Seed sd = seeds[e];
+		if (sd.frame == NO_SEED)
+			continue; // warp-uniform
+		const FrameDesc &fd = frames[sd.frame];
+		seed_eval(fd, (int)(sd.pixel % (unsigned)fd.w), (int)(sd.pixel / (unsigned)fd.w), sd.sig,
+			sd.noise, prm, patches[warp], triples[warp]);
 	}
 }
 
