@@ -43,8 +43,8 @@
 // aligned body starts on an odd cell is stored one cell to the right (its
 // shift).  Each ring row has a "full" mbarrier (lane 0's transaction bytes
 // plus lane 1's cp.async arrive) and an "empty" mbarrier on which each of the
-// four consumer warps arrives when it is done with the row.  The producer also
-// clears the S1/S2/CAND bit words of the rows it issues.  A block takes items
+// four consumer warps arrives when it is done with the row.  (The S1, S2 and
+// CAND planes are zeroed before the pass by zero_words_kernel.)  A block takes items
 // of BK_COLS x BK_ROWS pixels from a ticket counter (items of frames that
 // stopped are skipped there) and the ring runs straight through from one item
 // into the next.
@@ -382,12 +382,10 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 		}
 		const int4 it = items[t];
 		const FrameDesc &fd = frames[it.x];
-		const int w = fd.w, h = fd.h, words = fd.words, x0 = it.y, y0 = it.z;
+		const int w = fd.w, h = fd.h, x0 = it.y, y0 = it.z;
 		const int y1 = it.w; // items never cross a 32-row floor block
 		const double *clean = fd.clean;
 		const int mis = (int)(((uintptr_t)clean >> 3) & 1);
-		uint32_t *s1 = plane_ptr(fd, P_S1);
-		const long long plane = fd.plane;
 		for (int r = y0 - 1; r <= y1; ++r) {
 			const int slot = g & (BK_SLOTS - 1);
 			if (lane == 0)
@@ -417,14 +415,6 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 				mbar_arrive_cp_async(&R.full[slot]);
 			}
 			++g;
-			// Clear the S1, S2 and CAND words of the item's rows (16 words per
-			// plane per row).
-			if (r >= y0 && r < y1)
-				for (int q = lane; q < 48; q += 32) {
-					const int word = (x0 >> 5) + (q & 15);
-					if (word < words)
-						s1[(q >> 4) * plane + (long long)r * words + word] = 0u;
-				}
 		}
 	}
 }
@@ -450,13 +440,41 @@ __device__ __forceinline__ void load_quad(const double *row, int c, int shift, d
 	}
 }
 
-// Consumer warps of sig_bulk_kernel: returns false after a fault.
+// Columns x - 1 .. x + 4 of a ring row (x = the lane's first column, at cell
+// c + shift; c even, so every 16-byte load is aligned).
+__device__ __forceinline__ void load_six(const double *row, int c, int shift, double (&v)[6])
+{
+	if (shift == 0) {
+		const double2 a = *reinterpret_cast<const double2 *>(row + c);
+		const double2 b = *reinterpret_cast<const double2 *>(row + c + 2);
+		v[0] = row[c - 1];
+		v[1] = a.x;
+		v[2] = a.y;
+		v[3] = b.x;
+		v[4] = b.y;
+		v[5] = row[c + 4];
+	} else {
+		const double2 a = *reinterpret_cast<const double2 *>(row + c);
+		const double2 b = *reinterpret_cast<const double2 *>(row + c + 2);
+		const double2 d = *reinterpret_cast<const double2 *>(row + c + 4);
+		v[0] = a.x;
+		v[1] = a.y;
+		v[2] = b.x;
+		v[3] = b.y;
+		v[4] = d.x;
+		v[5] = d.y;
+	}
+}
+
+// Consumer warps of sig_bulk_kernel: lane ct of the four warps evaluates
+// columns x0 + 4 ct .. x0 + 4 ct + 3.  Returns false after a fault.
 __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__restrict__ frames,
 	const int4 *__restrict__ items, const DetectParams &prm, PreCand *pre, int *pre_counts)
 {
 	const double tmin2 = fmin(prm.thi2, prm.tlo2);
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int ct = warp * 32 + lane; // 0 .. 127
+	const int c0 = 2 + 4 * ct;       // cell of the lane's first column (before the row's shift)
 	const unsigned below = (1u << lane) - 1u;
 	int g = 0;
 	bool ok = true;
@@ -471,44 +489,37 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 		const int4 it = items[t];
 		const int f = it.x, x0 = it.y, y0 = it.z;
 		const FrameDesc &fd = frames[f];
-		const int w = fd.w, by = y0 / FLOOR_BLOCK;
-		const int bw = (w + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
-		// Pair sets p = 0, 1: columns xs[p] = x0 + 256 p + 2 ct and xs[p] + 1.
-		int xs[2];
-		unsigned ta[2], tb[2]; // high word of the block threshold (all ones: not a pixel)
-#pragma unroll
-		for (int p = 0; p < 2; ++p) {
-			xs[p] = x0 + BK_HALF * p + 2 * ct;
-			ta[p] = 0xffffffffu;
-			if (xs[p] < w) {
-				const int bx = xs[p] / FLOOR_BLOCK;
-				double T = fd.error ? fd.floors[by * bw + bx].thr
+		const int w = fd.w, x = x0 + 4 * ct;
+		// High word of the block threshold per column (all ones: not a pixel).
+		unsigned thr[4];
+		{
+			unsigned tv = 0xffffffffu;
+			if (x < w) {
+				const int bx = x / FLOOR_BLOCK, by = y0 / FLOOR_BLOCK;
+				const double T = fd.error ? fd.floors[by * ((w + FLOOR_BLOCK - 1) / FLOOR_BLOCK) + bx].thr
 					: model_threshold(fd, bx, by, prm.mode, tmin2);
-				ta[p] = hi_word(T >= 0 ? T : 0.0); // NaN lists everything
+				tv = hi_word(T >= 0 ? T : 0.0); // NaN lists everything
 			}
-			tb[p] = xs[p] + 1 < w ? ta[p] : 0xffffffffu;
+#pragma unroll
+			for (int i = 0; i < 4; ++i)
+				thr[i] = x + i < w ? tv : 0xffffffffu;
 		}
 		ok = __all_sync(0xffffffffu,
 			mbar_wait(&R.full[(g + 1) & (BK_SLOTS - 1)], ((g + 1) / BK_SLOTS) & 1, &R.abort));
 		if (!ok)
 			break;
-		// Row y0 - 1 (pair values) and row y0 (pair values and neighbours).
-		double qa[2], qb[2], ql[2], qr[2], upa[2], upb[2];
+		// Row y0 - 1 (values) and row y0 (values and neighbours), as quarters.
+		double q[4], up[4], ql, qr;
 		{
-			const int su = R.shift[g & (BK_SLOTS - 1)], sc = R.shift[(g + 1) & (BK_SLOTS - 1)];
-			const double *ru = R.c[g & (BK_SLOTS - 1)], *rc = R.c[(g + 1) & (BK_SLOTS - 1)];
+			double u[6], c[6];
+			load_six(R.c[g & (BK_SLOTS - 1)], c0, R.shift[g & (BK_SLOTS - 1)], u);
+			load_six(R.c[(g + 1) & (BK_SLOTS - 1)], c0, R.shift[(g + 1) & (BK_SLOTS - 1)], c);
+			ql = c[0] * 0.25;
+			qr = c[5] * 0.25;
 #pragma unroll
-			for (int p = 0; p < 2; ++p) {
-				const int c = 2 + BK_HALF * p + 2 * ct;
-				double ul, ua, ub, ur;
-				load_quad(ru, c, su, ul, ua, ub, ur);
-				load_quad(rc, c, sc, ql[p], qa[p], qb[p], qr[p]);
-				qa[p] *= 0.25;
-				qb[p] *= 0.25;
-				ql[p] *= 0.25;
-				qr[p] *= 0.25;
-				upa[p] = qa[p] - ua * 0.25;
-				upb[p] = qb[p] - ub * 0.25;
+			for (int i = 0; i < 4; ++i) {
+				q[i] = c[i + 1] * 0.25;
+				up[i] = q[i] - u[i + 1] * 0.25;
 			}
 		}
 		__syncwarp();
@@ -524,48 +535,39 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 			ok = __all_sync(0xffffffffu, mbar_wait(&R.full[sd], (gd / BK_SLOTS) & 1, &R.abort));
 			if (!ok)
 				break;
-			double nl[2], na[2], nb[2], nr[2];
-			{
-				const int s = R.shift[sd];
-#pragma unroll
-				for (int p = 0; p < 2; ++p)
-					load_quad(R.c[sd], 2 + BK_HALF * p + 2 * ct, s, nl[p], na[p], nb[p], nr[p]);
-			}
+			double n[6];
+			load_six(R.c[sd], c0, R.shift[sd], n);
 			__syncwarp();
 			if (lane == 0)
 				mbar_arrive(&R.empty[sd]); // row y + 1 is in registers
-			const long long rowpix = (long long)y * w;
+			// Horizontal differences: left(x+i) = h[i], right(x+i) = -h[i+1].
+			double h[5];
+			h[0] = q[0] - ql;
 #pragma unroll
-			for (int p = 0; p < 2; ++p) {
-				const double qda = na[p] * 0.25, qdb = nb[p] * 0.25;
-				const double da = qa[p] - qda, db = qb[p] - qdb;
-				const double hl = qa[p] - ql[p], hab = qa[p] - qb[p], hr = qb[p] - qr[p];
-				const double lap_a = (pos_ub(upa[p] + hl) + pos_ub(upa[p] + hab)) +
-					(pos_ub(da + hl) + pos_ub(da + hab));
-				const double lap_b = (pos_ub(upb[p] - hab) + pos_ub(upb[p] + hr)) +
-					(pos_ub(db - hab) + pos_ub(db + hr));
-				const bool pa = hi_word(lap_a) >= ta[p], pb = hi_word(lap_b) >= tb[p];
-				const unsigned ba = __ballot_sync(0xffffffffu, pa);
-				if (ba) {
-					if (pa)
-						region[cnt + __popc(ba & below)] =
-							PreCand{(unsigned)(rowpix + xs[p]), (unsigned)f, lap_a};
-					cnt += __popc(ba);
+			for (int i = 0; i < 3; ++i)
+				h[i + 1] = q[i] - q[i + 1];
+			h[4] = q[3] - qr;
+			const long long pix0 = (long long)y * w + x;
+#pragma unroll
+			for (int i = 0; i < 4; ++i) {
+				const double qd = n[i + 1] * 0.25;
+				const double d = q[i] - qd;
+				const double lft = i == 0 ? h[0] : -h[i], rgt = i == 3 ? h[4] : h[i + 1];
+				const double lap = (pos_ub(up[i] + lft) + pos_ub(up[i] + rgt)) +
+					(pos_ub(d + lft) + pos_ub(d + rgt));
+				const bool pass = hi_word(lap) >= thr[i];
+				const unsigned bal = __ballot_sync(0xffffffffu, pass);
+				if (bal) {
+					if (pass)
+						region[cnt + __popc(bal & below)] =
+							PreCand{(unsigned)(pix0 + i), (unsigned)f, lap};
+					cnt += __popc(bal);
 				}
-				const unsigned bb = __ballot_sync(0xffffffffu, pb);
-				if (bb) {
-					if (pb)
-						region[cnt + __popc(bb & below)] =
-							PreCand{(unsigned)(rowpix + xs[p] + 1), (unsigned)f, lap_b};
-					cnt += __popc(bb);
-				}
-				upa[p] = -da;
-				upb[p] = -db;
-				qa[p] = qda;
-				qb[p] = qdb;
-				ql[p] = nl[p] * 0.25;
-				qr[p] = nr[p] * 0.25;
+				up[i] = -d;
+				q[i] = qd;
 			}
+			ql = n[0] * 0.25;
+			qr = n[5] * 0.25;
 		}
 		if (!ok)
 			break;

@@ -3,7 +3,7 @@
 //
 // HBM layout of one call (all per frame, frames back to back):
 //   clean      float64 [h][w]      working pixels; the caller's output buffer
-//   bit planes uint32  [N_PLANES][h][words], words = ceil(w / 32); bit b of
+//   bit planes uint32  [N_PLANES][frames][h][words], words = ceil(w / 32); bit b of
 //              word (y, k) is pixel (y, 32 k + b); padding bits are zero
 //   targets    uint2   {frame, pixel} list of replacement targets
 #pragma once
@@ -40,6 +40,8 @@ enum Plane {
 	P_FRESH,  // pixels the last growth step added to the mask
 	N_PLANES
 };
+
+static_assert(P_S2 == P_S1 + 1 && P_CAND == P_S1 + 2, "S1, S2 and CAND are zeroed as one range");
 
 constexpr double FINE_FLOOR = 0.01;   // reference src/filters.cuh:21
 constexpr double SIGNAL_FLOOR = 1e-5; // reference src/filters.cuh:22
@@ -92,7 +94,9 @@ struct FrameDesc {
 	uint32_t *bits;    // N_PLANES planes of `plane` words
 	BlockFloor *floors; // the frame's block floors, row-major by block (null: none)
 	double gain, rn, bg;
-	long long plane;   // words per plane = h * words
+	long long plane;   // words per plane of this frame = h * words
+	long long pstride; // words from one plane to the next (planes of all frames of a
+	                   // batch are interleaved plane by plane, so pstride >= plane)
 	int w, h, words, has_bg;
 };
 
@@ -126,7 +130,7 @@ struct Control {
 
 CB_HD uint32_t *plane_ptr(const FrameDesc &f, int p)
 {
-	return f.bits + (long long)p * f.plane;
+	return f.bits + (long long)p * f.pstride;
 }
 
 CB_HD bool test_bit(const uint32_t *plane, int words, int x, int y)

@@ -118,14 +118,15 @@ static cusmic_tuning tuning_for(size_t total_px)
 // Host description of one batch.
 struct Layout {
 	std::vector<FrameDesc> frames;
-	std::vector<long long> bit_off; // word offset of each frame's planes
+	std::vector<long long> bit_off; // word offset of each frame within a plane
 	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, first threshold of the frame}
 	std::vector<FloorJob> jobs; // floor blocks of each distinct error map
 	std::vector<long long> thr_base; // per frame: first floor of its blocks
 	long long nthr = 0;
 	std::vector<int2> rows;
 	std::vector<long long> offsets; // first output pixel of each frame
-	long long total_words = 0;
+	long long total_words = 0;  // all planes
+	long long plane_words = 0;  // one plane of every frame
 	size_t total_px = 0;
 	DetectParams prm{};
 	int maxiter = 0;
@@ -339,7 +340,7 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		d.bits = nullptr;
 		L.bit_off[f] = words;
 		L.offsets.push_back((long long)px);
-		words += (long long)N_PLANES * d.plane;
+		words += d.plane;
 		px += (size_t)d.w * d.h;
 		for (int y = 0; y < d.h; ++y)
 			L.rows.push_back(make_int2((int)f, y));
@@ -368,7 +369,11 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 				L.bulk.push_back(make_int4((int)f, tx, ty, std::min(ty + rows_per_item, d.h)));
 	}
 	L.total_px = px;
-	L.total_words = words;
+	// Planes padded to 4 words, so every plane starts on a 16-byte boundary.
+	L.plane_words = (words + 3) & ~3ll;
+	L.total_words = (long long)N_PLANES * L.plane_words;
+	for (FrameDesc &d : L.frames)
+		d.pstride = L.plane_words;
 	return L;
 }
 
@@ -481,6 +486,13 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	const int nbulk = (int)L.bulk.size();
 	const int cap = di.sms * L.tune.dense_blocks_per_sm, sparse = di.sms * L.tune.sparse_blocks_per_sm;
 	const int rowb = L.tune.row_blocks_per_sm;
+	{
+		// S1, S2 and CAND of every frame: 3 contiguous planes of 16-byte words.
+		const long long n16 = 3 * L.plane_words / 4;
+		const long long blocks = (n16 + 255) / 256 < di.sms * 4 ? (n16 + 255) / 256 : di.sms * 4;
+		zero_words_kernel<<<(int)blocks, 256, 0, s>>>(
+			reinterpret_cast<uint4 *>(ws.bits.p + P_S1 * L.plane_words), n16);
+	}
 	sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
 	mark(rec, K_SIGRAW);
@@ -1188,6 +1200,7 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 		fd.h = h;
 		fd.words = (w + 31) / 32;
 		fd.plane = L.plane;
+		fd.pstride = L.plane;
 		fd.has_bg = im->background != nullptr || !std::isnan(o->background);
 		DetectParams prm{};
 		prm.contrast = o->contrast;

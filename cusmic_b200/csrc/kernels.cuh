@@ -71,6 +71,15 @@ __device__ __forceinline__ void set_flag(unsigned long long *flag)
 		*(volatile unsigned long long *)flag = 1;
 }
 
+// Zero n 16-byte words (the S1, S2 and CAND planes of all frames before a
+// detection pass: they are contiguous in the plane-major layout).
+__global__ void __launch_bounds__(256) zero_words_kernel(uint4 *p, long long n)
+{
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+	     i += (long long)gridDim.x * blockDim.x)
+		p[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
 	unsigned long long cand_cap)
 {
