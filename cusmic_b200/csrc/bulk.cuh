@@ -529,6 +529,7 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 		}
 		PreCand *region = pre + ((long long)t * BK_CWARPS + warp) * BK_REGION;
 		int cnt = 0;
+#pragma unroll 2
 		for (int y = y0; y < y1; ++y) {
 			const int gd = g + 2 + (y - y0); // ring row of y + 1
 			const int sd = gd & (BK_SLOTS - 1);
@@ -548,26 +549,32 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 				h[i + 1] = q[i] - q[i + 1];
 			h[4] = q[3] - qr;
 			const long long pix0 = (long long)y * w + x;
+			// The four columns' Laplacians first (independent chains), then
+			// the list appends.
+			double lap[4];
 #pragma unroll
 			for (int i = 0; i < 4; ++i) {
 				const double qd = n[i + 1] * 0.25;
 				const double d = q[i] - qd;
 				const double lft = i == 0 ? h[0] : -h[i], rgt = i == 3 ? h[4] : h[i + 1];
-				const double lap = (pos_ub(up[i] + lft) + pos_ub(up[i] + rgt)) +
+				lap[i] = (pos_ub(up[i] + lft) + pos_ub(up[i] + rgt)) +
 					(pos_ub(d + lft) + pos_ub(d + rgt));
-				const bool pass = hi_word(lap) >= thr[i];
-				const unsigned bal = __ballot_sync(0xffffffffu, pass);
-				if (bal) {
-					if (pass)
-						region[cnt + __popc(bal & below)] =
-							PreCand{(unsigned)(pix0 + i), (unsigned)f, lap};
-					cnt += __popc(bal);
-				}
 				up[i] = -d;
 				q[i] = qd;
 			}
 			ql = n[0] * 0.25;
 			qr = n[5] * 0.25;
+#pragma unroll
+			for (int i = 0; i < 4; ++i) {
+				const bool pass = hi_word(lap[i]) >= thr[i];
+				const unsigned bal = __ballot_sync(0xffffffffu, pass);
+				if (bal) {
+					if (pass)
+						region[cnt + __popc(bal & below)] =
+							PreCand{(unsigned)(pix0 + i), (unsigned)f, lap[i]};
+					cnt += __popc(bal);
+				}
+			}
 		}
 		if (!ok)
 			break;
