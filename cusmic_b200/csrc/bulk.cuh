@@ -9,10 +9,10 @@
 //    32 x 32 block, turned into a threshold T = 2 min(cr, nb) (1 - 1e-12) x
 //    floor.  With an error map floor_kernel takes min(max(error, 0)) over the
 //    block (NaN counts as 0), once for each distinct map.  With the noise
-//    model (src/filters.cuh:107-123) prepare_kernel stores the smallest clean
-//    value of the block (as an ordered key; holes excluded, the hole fill
-//    lowers it) and the block's largest gain and smallest read noise when
-//    they are maps.  Between passes only replacement changes clean,
+//    model (src/filters.cuh:107-123) it stores, after the hole fill, the
+//    smallest clean value of the block (as an ordered key) and the block's
+//    largest gain and smallest read noise when they are maps.  Between passes
+//    only replacement changes clean,
 //    and replace_kernel lowers the key of the block it writes into, so the key
 //    stays a lower bound of the block's values.  Every 5 x 5 median window of
 //    a block lies in the block's 3 x 3 neighbourhood of blocks (border-mapped
@@ -113,10 +113,10 @@ struct PreCand {
 	double lap;
 };
 
-// One 32 x 32 block of an error map whose threshold floor_kernel computes
-// (frames that share a map share its thresholds).
+// One 32 x 32 block whose floor floor_kernel computes: kind 0 = an error map
+// (frames that share a map share its thresholds), 1 = a noise-model frame.
 struct FloorJob {
-	int frame, x0, y0, pad;
+	int frame, x0, y0, kind;
 	long long out; // index into the threshold array
 };
 
@@ -248,8 +248,10 @@ CB_HD BulkRow bulk_row(int w, int h, int lm, int mis, int x0, int r)
 	return b;
 }
 
-// Error-map floors of 32 x 32 blocks (see the head of this file), for each
-// distinct map; one warp per block, one lane per column, all 32 rows in flight.
+// Floors of 32 x 32 blocks (see the head of this file): of each distinct
+// error map, and (after the hole fill, when every clean value is finite) of
+// each noise-model frame.  One warp per block, one lane per column, all 32
+// rows in flight.
 __global__ void __launch_bounds__(256)
 floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
 	DetectParams prm, BlockFloor *floors)
@@ -262,6 +264,34 @@ floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ 
 		const FrameDesc &fd = frames[jb.frame];
 		const int w = fd.w, x = jb.x0 + lane;
 		const int n = (jb.y0 + FLOOR_BLOCK < fd.h ? jb.y0 + FLOOR_BLOCK : fd.h) - jb.y0;
+		if (jb.kind) { // noise model: ordered keys of clean, -gain, read noise
+			const long long at = (long long)jb.y0 * w + x;
+			unsigned long long key = ~0ull, gkey = ~0ull, rkey = ~0ull;
+			double v[FLOOR_BLOCK];
+#pragma unroll
+			for (int k = 0; k < FLOOR_BLOCK; ++k)
+				v[k] = x < w && k < n ? fd.clean[at + (long long)k * w] : 0.0;
+#pragma unroll
+			for (int k = 0; k < FLOOR_BLOCK; ++k)
+				if (x < w && k < n)
+					key = min(key, order_key(v[k]));
+			if (x < w && (fd.gain_map || fd.rn_map))
+				for (int k = 0; k < n; ++k) {
+					if (fd.gain_map)
+						gkey = min(gkey, order_key(-fd.gain_map[at + (long long)k * w]));
+					if (fd.rn_map)
+						rkey = min(rkey, order_key(fd.rn_map[at + (long long)k * w]));
+				}
+#pragma unroll
+			for (int o = 16; o; o >>= 1) {
+				key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+				gkey = min(gkey, __shfl_xor_sync(0xffffffffu, gkey, o));
+				rkey = min(rkey, __shfl_xor_sync(0xffffffffu, rkey, o));
+			}
+			if (lane == 0)
+				floors[jb.out] = BlockFloor{0.0, key, gkey, rkey};
+			continue;
+		}
 		const double *col = fd.error + (long long)jb.y0 * w + x;
 		double v[FLOOR_BLOCK];
 #pragma unroll

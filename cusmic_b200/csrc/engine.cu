@@ -120,7 +120,7 @@ struct Layout {
 	std::vector<FrameDesc> frames;
 	std::vector<long long> bit_off; // word offset of each frame within a plane
 	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, first threshold of the frame}
-	std::vector<FloorJob> jobs; // floor blocks of each distinct error map
+	std::vector<FloorJob> jobs; // floor blocks of each distinct error map and noise-model frame
 	std::vector<long long> thr_base; // per frame: first floor of its blocks
 	long long nthr = 0;
 	std::vector<int2> rows;
@@ -354,13 +354,12 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 					base = m.second;
 		if (base < 0) {
 			base = L.nthr;
-			if (d.error) {
+			if (d.error)
 				maps[d.error].push_back({(int)f, base});
-				for (int by = 0; by < bh; ++by)
-					for (int bx = 0; bx < bw; ++bx)
-						L.jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK, 0,
-							base + (long long)by * bw + bx});
-			}
+			for (int by = 0; by < bh; ++by)
+				for (int bx = 0; bx < bw; ++bx)
+					L.jobs.push_back(FloorJob{(int)f, bx * FLOOR_BLOCK, by * FLOOR_BLOCK,
+						d.error ? 0 : 1, base + (long long)by * bw + bx});
 			L.nthr += (long long)bw * bh;
 		}
 		L.thr_base[f] = base;
@@ -529,16 +528,15 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		mark(rec, K_COPY);
 		return;
 	}
-	// All-ones floor keys: prepare_kernel and the fill lower them.  Zero bit
-	// planes: prepare_kernel writes HOLE, EXCL and DONOR.
-	check(cudaMemsetAsync(ws.floors.p, 0xff, (size_t)L.nthr * sizeof(BlockFloor), s));
+	// Zero bit planes: prepare_kernel writes HOLE, EXCL and DONOR.
 	check(cudaMemsetAsync(ws.bits.p, 0, (size_t)L.total_words * sizeof(uint32_t), s));
 	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
 		nrows);
 	mark(rec, K_PREPARE);
 	fill_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows);
 	mark(rec, K_FILL);
-	// Error-map thresholds.
+	// Block floors (error-map thresholds; noise-model keys of the filled
+	// frames, which replacement keeps as lower bounds).
 	if (!L.jobs.empty()) {
 		const int nj = (int)L.jobs.size(), cap = di.sms * 8;
 		floor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p, ws.jobs.p,

@@ -110,16 +110,6 @@ __device__ __forceinline__ double order_value(unsigned long long k)
 	return __longlong_as_double((long long)((k >> 63) ? k ^ (1ull << 63) : ~k));
 }
 
-// Lower *target to the warp's smallest key (one atomic per warp).
-__device__ __forceinline__ void warp_min_key(unsigned long long *target, unsigned long long k)
-{
-#pragma unroll
-	for (int o = 16; o; o >>= 1)
-		k = min(k, __shfl_xor_sync(0xffffffffu, k, o));
-	if ((threadIdx.x & 31) == 0 && k != ~0ull)
-		atomicMin(target, k);
-}
-
 // Reference src/image.cuh:24-48: holes, exclusions, clean = data (+ bg), the
 // static donor plane (the reference's is_donor with an empty mask) and the
 // per-frame facts the initial fill needs (src/cleaner.cuh:78-100).  A warp
@@ -127,100 +117,115 @@ __device__ __forceinline__ void warp_min_key(unsigned long long *target, unsigne
 // in flight per SM to approach the HBM bandwidth.
 constexpr int ROW_UNROLL = 4;
 
+// One row of prepare_kernel for the frame kinds that occur: MASK = input
+// mask, BGMAP = background map.  Descriptor fields are held in registers (the
+// stores below go through pointers the compiler cannot prove distinct from
+// them).
+template <bool MASK, bool BGMAP>
+__device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st, int y)
+{
+	const int lane = threadIdx.x & 31;
+	const int w = fd.w, words = fd.words;
+	const long long rowpix = (long long)y * w, roww = (long long)y * words;
+	const double *__restrict__ data = fd.data + rowpix;
+	// MASK / BGMAP false: the frame has none; true: it may have one.
+	const uint8_t *__restrict__ mask = MASK && fd.mask ? fd.mask + rowpix : nullptr;
+	const double *__restrict__ bgmap = BGMAP && fd.bg_map ? fd.bg_map + rowpix : nullptr;
+	double *__restrict__ clean = fd.clean + rowpix;
+	const double bgv = fd.bg;
+	const bool has_bg = fd.has_bg;
+	uint32_t *hole_plane = plane_ptr(fd, P_HOLE) + roww, *excl_plane = plane_ptr(fd, P_EXCL) + roww;
+	uint32_t *donor_plane = plane_ptr(fd, P_DONOR) + roww;
+	uint32_t any_hole = 0, any_allowed = 0, any_finite = 0;
+	for (int seg = 0; seg * 1024 < w; ++seg) {
+		uint32_t my_h = 0, my_e = 0, my_d = 0;
+		for (int c0 = 0; c0 < 32; c0 += ROW_UNROLL) {
+			const int xb = seg * 1024 + c0 * 32;
+			if (xb >= w)
+				break; // warp-uniform
+			double d[ROW_UNROLL], bg[ROW_UNROLL];
+			bool m[ROW_UNROLL];
+#pragma unroll
+			for (int u = 0; u < ROW_UNROLL; ++u) {
+				const int x = xb + 32 * u + lane;
+				d[u] = 0;
+				bg[u] = bgv;
+				m[u] = false;
+				if (x < w) {
+					d[u] = data[x];
+					if (MASK && mask)
+						m[u] = mask[x] != 0;
+					if (BGMAP && bgmap)
+						bg[u] = bgmap[x];
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < ROW_UNROLL; ++u) {
+				const int x0 = xb + 32 * u;
+				const int x = x0 + lane;
+				const bool valid = x < w;
+				bool hole = false, ok = false, donor = false;
+				double c = 0;
+				if (valid) {
+					hole = !isfinite(d[u]);
+					ok = !hole && !m[u];
+					c = hole ? 0 : d[u];
+					if (has_bg)
+						c += 1 * bg[u];
+					clean[x] = c;
+					donor = ok && isfinite(c);
+				}
+				const uint32_t hw = __ballot_sync(0xffffffffu, hole);
+				const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
+				const uint32_t dw = __ballot_sync(0xffffffffu, donor);
+				any_allowed |= __ballot_sync(0xffffffffu, ok);
+				any_finite |= dw;
+				any_hole |= hw;
+				if (lane == c0 + u) {
+					my_h = hw;
+					my_e = ew;
+					my_d = dw;
+				}
+			}
+		}
+		const int k = seg * 32 + lane;
+		if (k < words) {
+			hole_plane[k] = my_h;
+			excl_plane[k] = my_e;
+			donor_plane[k] = my_d;
+		}
+	}
+	if (lane == 0) {
+		if (any_hole)
+			set_flag(&st.holes);
+		if (any_allowed)
+			set_flag(&st.allowed);
+		if (any_finite)
+			set_flag(&st.finite);
+	}
+}
+
 // One warp per row (grid-stride over the row list), in segments of 32 words
 // (1024 pixels): lane j keeps the HOLE, EXCL and DONOR words of the
 // segment's word j, so each plane gets one coalesced store per segment.  The
 // other planes were zeroed before the kernel.  Holes are not listed: the hole
 // fill scans the HOLE plane.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
 	int nrows)
 {
-	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
 	for (int r = gw; r < nrows; r += nw) {
 		const int2 item = rows[r];
 		const FrameDesc &fd = frames[item.x];
-		const int w = fd.w, y = item.y, words = fd.words;
-		const long long rowpix = (long long)y * w, roww = (long long)y * words;
-		uint32_t any_hole = 0, any_allowed = 0, any_finite = 0;
-		for (int seg = 0; seg * 1024 < w; ++seg) {
-			uint32_t my_h = 0, my_e = 0, my_d = 0;
-			for (int c0 = 0; c0 < 32; c0 += ROW_UNROLL) {
-				const int xb = seg * 1024 + c0 * 32;
-				if (xb >= w)
-					break; // warp-uniform
-				double d[ROW_UNROLL], bg[ROW_UNROLL];
-				bool m[ROW_UNROLL];
-#pragma unroll
-				for (int u = 0; u < ROW_UNROLL; ++u) {
-					const int x = xb + 32 * u + lane;
-					d[u] = 0;
-					bg[u] = fd.bg;
-					m[u] = false;
-					if (x < w) {
-						d[u] = fd.data[rowpix + x];
-						if (fd.mask)
-							m[u] = fd.mask[rowpix + x] != 0;
-						if (fd.bg_map)
-							bg[u] = fd.bg_map[rowpix + x];
-					}
-				}
-#pragma unroll
-				for (int u = 0; u < ROW_UNROLL; ++u) {
-					const int x0 = xb + 32 * u;
-					const int x = x0 + lane;
-					const bool valid = x < w;
-					bool hole = false, ok = false, donor = false;
-					double c = 0;
-					if (valid) {
-						hole = !isfinite(d[u]);
-						ok = !hole && !m[u];
-						c = hole ? 0 : d[u];
-						if (fd.has_bg)
-							c += 1 * bg[u];
-						fd.clean[rowpix + x] = c;
-						donor = ok && isfinite(c);
-					}
-					// Noise-model frames: block floors of clean (holes are
-					// filled later, and the fill lowers the floors itself), of
-					// -gain and of the read noise.
-					if (fd.floors && !fd.error && x0 < w) {
-						BlockFloor &bf = fd.floors[(y >> 5) * ((w + 31) >> 5) + (x0 >> 5)];
-						warp_min_key(&bf.key, valid && !hole ? order_key(c) : ~0ull);
-						if (fd.gain_map)
-							warp_min_key(&bf.gkey, valid ? order_key(-fd.gain_map[rowpix + x]) : ~0ull);
-						if (fd.rn_map)
-							warp_min_key(&bf.rkey, valid ? order_key(fd.rn_map[rowpix + x]) : ~0ull);
-					}
-					const uint32_t hw = __ballot_sync(0xffffffffu, hole);
-					const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
-					const uint32_t dw = __ballot_sync(0xffffffffu, donor);
-					any_allowed |= __ballot_sync(0xffffffffu, ok);
-					any_finite |= dw;
-					any_hole |= hw;
-					if (lane == c0 + u) {
-						my_h = hw;
-						my_e = ew;
-						my_d = dw;
-					}
-				}
-			}
-			const int k = seg * 32 + lane;
-			if (k < words) {
-				plane_ptr(fd, P_HOLE)[roww + k] = my_h;
-				plane_ptr(fd, P_EXCL)[roww + k] = my_e;
-				plane_ptr(fd, P_DONOR)[roww + k] = my_d;
-			}
-		}
-		if (lane == 0) {
-			if (any_hole)
-				set_flag(&state[item.x].holes);
-			if (any_allowed)
-				set_flag(&state[item.x].allowed);
-			if (any_finite)
-				set_flag(&state[item.x].finite);
-		}
+		FrameState &st = state[item.x];
+		const bool mask = fd.mask, bgmap = fd.bg_map;
+		if (mask && !bgmap)
+			prepare_row<true, false>(fd, st, item.y);
+		else if (!mask && !bgmap)
+			prepare_row<false, false>(fd, st, item.y);
+		else
+			prepare_row<true, true>(fd, st, item.y);
 	}
 }
 
