@@ -172,6 +172,7 @@ struct Workspace {
 	// Host-API staging of inputs and outputs.
 	DevBuf<double> hdata, herror, hgain, hrn, hbg, hclean;
 	DevBuf<uint8_t> hmask, hout;
+	DevBuf<unsigned> hflags; // failed map checks of the host entry point
 };
 
 static std::mutex pool_mu;
@@ -638,15 +639,6 @@ static void run_device(const cusmic_image *ims, size_t nf, const cusmic_options 
 	finish(*ws, nf, s, passes);
 }
 
-// Reference src/api.cu:107-114.
-static void check_values(const double *data, size_t n, const char *name, int minimum)
-{
-	for (size_t i = 0; data && i < n; ++i)
-		if (!std::isfinite(data[i]) || (minimum == 1 && data[i] <= 0) ||
-			(minimum == 0 && data[i] < 0))
-			throw InvalidArgument(name);
-}
-
 } // namespace cb
 
 using namespace cb;
@@ -673,13 +665,6 @@ extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, d
 	return guarded([&] {
 		check_arguments(im, 1, o, nullptr, clean, mask, true);
 		const size_t n = im->width * im->height;
-		if (im->error)
-			check_values(im->error, n, "error must be finite and positive", 1);
-		else {
-			check_values(im->gain, n, "gain must be finite and positive", 1);
-			check_values(im->readnoise, n, "read noise must be finite and nonnegative", 0);
-		}
-		check_values(im->background, n, "background must be finite", -1);
 
 		int dev;
 		check(cudaGetDevice(&dev));
@@ -710,9 +695,38 @@ extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, d
 			gpu.mask = ws->hmask.p;
 		}
 		DeviceInfo di = device_info(dev);
+		// The maps' contents are checked on the device (the reference checks
+		// them on the host first, src/api.cu:161-168): the flags are read
+		// before any output is copied back, so a failing call leaves the
+		// outputs untouched and reports the first failing map, in the
+		// reference's order.
+		ws->hflags.ensure(1);
+		check(cudaMemsetAsync(ws->hflags.p, 0, sizeof(unsigned), s));
+		auto validate = [&](const double *p, int minimum, unsigned bit) {
+			if (!p)
+				return;
+			const long long blocks = ((long long)n + 255) / 256 < di.sms * 4 ? ((long long)n + 255) / 256
+											   : di.sms * 4;
+			validate_kernel<<<(int)blocks, 256, 0, s>>>(p, (long long)n, minimum, ws->hflags.p, bit);
+		};
+		validate(gpu.error, 1, 1u);
+		validate(gpu.gain, 1, 2u);
+		validate(gpu.readnoise, 0, 4u);
+		validate(gpu.background, -1, 8u);
 		Layout L = make_layout(&gpu, 1, *o, nullptr, ws->hclean.p, ws->hout.p, di);
 		upload(*ws, L, s);
 		enqueue_plain(*ws, L, di, s);
+		unsigned bad = 0;
+		check(cudaMemcpyAsync(&bad, ws->hflags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+		check(cudaStreamSynchronize(s));
+		if (bad & 1u)
+			throw InvalidArgument("error must be finite and positive");
+		if (bad & 2u)
+			throw InvalidArgument("gain must be finite and positive");
+		if (bad & 4u)
+			throw InvalidArgument("read noise must be finite and nonnegative");
+		if (bad & 8u)
+			throw InvalidArgument("background must be finite");
 		finish(*ws, 1, s);
 		check(cudaMemcpy(clean, ws->hclean.p, n * sizeof(double), cudaMemcpyDeviceToHost));
 		check(cudaMemcpy(mask, ws->hout.p, n, cudaMemcpyDeviceToHost));

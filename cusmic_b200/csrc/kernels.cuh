@@ -71,6 +71,23 @@ __device__ __forceinline__ void set_flag(unsigned long long *flag)
 		*(volatile unsigned long long *)flag = 1;
 }
 
+// Map validation of the host entry point on the device (reference
+// src/api.cu:107-114 runs it on the host): sets `bit` in *flags if any of the
+// n values is not finite, or (minimum 1) not positive, or (minimum 0)
+// negative.
+__global__ void __launch_bounds__(256)
+validate_kernel(const double *__restrict__ v, long long n, int minimum, unsigned *flags, unsigned bit)
+{
+	bool bad = false;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+	     i += (long long)gridDim.x * blockDim.x) {
+		const double x = v[i];
+		bad |= !isfinite(x) || (minimum == 1 && x <= 0) || (minimum == 0 && x < 0);
+	}
+	if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0)
+		atomicOr(flags, bit);
+}
+
 // Zero n 16-byte words (the S1, S2 and CAND planes of all frames before a
 // detection pass: they are contiguous in the plane-major layout).
 __global__ void __launch_bounds__(256) zero_words_kernel(uint4 *p, long long n)

@@ -362,3 +362,31 @@ def test_structured_scenes_heavy_masks(cuda, oracle, seed):
     frame = dict(data=data, mask=mask, gain=float(rng.uniform(1, 3)), readnoise=float(rng.uniform(2, 8)))
     check_against_oracle(oracle, [frame], dict(SETTINGS, border=mode, gain=frame["gain"],
                                                readnoise=frame["readnoise"]))
+
+
+@pytest.mark.parametrize("maps,message", [
+    (dict(error=[1, 1, 0, 1]), "error must be finite and positive"),
+    (dict(error=[1, math.inf, 1, 1]), "error must be finite and positive"),
+    (dict(gain=[1, 1, -1, 1]), "gain must be finite and positive"),
+    (dict(gain=[1, 1, 1, 1], readnoise=[0, -1, 0, 0]), "read noise must be finite and nonnegative"),
+    (dict(gain=[1, 1, 1, 1], background=[1, 1, math.nan, 1]), "background must be finite"),
+    (dict(error=[1, 0, 1, 1], background=[1, math.nan, 1, 1]), "error must be finite and positive"),
+])
+def test_host_api_map_contents(cuda, maps, message):
+    """reference src/api.cu:107-114,161-168: map contents are validated, the
+    first failing map (error, gain, read noise, background) is reported and
+    the host outputs stay untouched."""
+    from cusmic_b200 import _native
+    keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in maps.items()}
+    data = np.array([10.0, 11, 12, 13])
+    ptr = lambda k: keep[k].ctypes.data if k in keep else None
+    im = _native.Image(data.ctypes.data, ptr("error"), ptr("gain"), ptr("readnoise"),
+                       ptr("background"), None, 2, 2)
+    o = cabi.options(gain=1.0 if "error" not in maps else math.nan)
+    clean = np.full(4, 9.0)
+    mask = np.full(4, 9, np.uint8)
+    msg = ctypes.create_string_buffer(128)
+    st = _native.lib().remove_cosmics(ctypes.byref(im), ctypes.byref(o), clean.ctypes.data,
+                                      mask.ctypes.data, msg, 128)
+    assert st == _native.CUSMIC_INVALID and msg.value.decode() == message
+    assert (clean == 9).all() and (mask == 9).all()
