@@ -36,12 +36,13 @@ enum Plane {
 	P_S1,     // significance > cr_threshold
 	P_S2,     // significance > neighbor_threshold
 	P_CAND,   // seed: S1, not excluded, contrast test passed
-	P_CRMASK, // cumulative cosmic-ray mask
 	P_FRESH,  // pixels the last growth step added to the mask
+	P_CRMASK, // cumulative cosmic-ray mask
 	N_PLANES
 };
 
-static_assert(P_S2 == P_S1 + 1 && P_CAND == P_S1 + 2, "S1, S2 and CAND are zeroed as one range");
+static_assert(P_S2 == P_S1 + 1 && P_CAND == P_S1 + 2 && P_FRESH == P_S1 + 3,
+	"S1, S2, CAND and FRESH are zeroed as one range before each pass");
 
 constexpr double FINE_FLOOR = 0.01;   // reference src/filters.cuh:21
 constexpr double SIGNAL_FLOOR = 1e-5; // reference src/filters.cuh:22
@@ -93,6 +94,7 @@ struct FrameDesc {
 	uint8_t *mask_out; // uint8 output mask
 	uint32_t *bits;    // N_PLANES planes of `plane` words
 	BlockFloor *floors; // the frame's block floors, row-major by block (null: none)
+	uint32_t *rowcand;  // per row: nonzero when the row got a CAND bit this pass (null: none)
 	double gain, rn, bg;
 	long long plane;   // words per plane of this frame = h * words
 	long long pstride; // words from one plane to the next (planes of all frames of a
@@ -108,7 +110,8 @@ struct FrameState {
 	unsigned int passes;  // detection passes run
 	unsigned int fault;   // a bounded wait inside a kernel ran out (the frame stopped)
 	// Nonzero-only facts (set to 1 by many warps, never counted):
-	unsigned long long todo, donors;          // this pass: any new pixel, any donor left
+	unsigned long long todo;                  // this pass: any new pixel
+	long long donors_left;                    // static donors not in the mask (counted)
 	unsigned long long holes, allowed, finite; // any hole, any allowed pixel, any finite donor
 };
 

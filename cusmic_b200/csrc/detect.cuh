@@ -668,8 +668,11 @@ __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, dou
 	if (lane == 0) {
 		double fine = (med3c - med7) / noise;
 		fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
-		if (sig / fine > prm.contrast)
+		if (sig / fine > prm.contrast) {
 			atomicOr(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
+			if (fd.rowcand)
+				fd.rowcand[y] = 1u;
+		}
 	}
 }
 

@@ -119,6 +119,8 @@ static cusmic_tuning tuning_for(size_t total_px)
 struct Layout {
 	std::vector<FrameDesc> frames;
 	std::vector<long long> bit_off; // word offset of each frame within a plane
+	std::vector<long long> row_off; // first row of each frame in the row marks
+	long long row_words = 0;        // row marks of all frames, padded to 4
 	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, first threshold of the frame}
 	std::vector<FloorJob> jobs; // floor blocks of each distinct error map and noise-model frame
 	std::vector<long long> thr_base; // per frame: first floor of its blocks
@@ -156,6 +158,7 @@ struct Workspace {
 	DevBuf<FrameState> state;
 	DevBuf<int2> rows;
 	DevBuf<uint32_t> bits;
+	DevBuf<uint32_t> rowcand;
 	DevBuf<uint2> targets;
 	DevBuf<uint8_t> radius; // per target: window radius of its last replacement
 	DevBuf<uint2> cands;
@@ -340,6 +343,8 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		d.has_bg = im.background != nullptr || !std::isnan(s.bg);
 		d.bits = nullptr;
 		L.bit_off[f] = words;
+		L.row_off.push_back(L.row_words);
+		L.row_words += d.h;
 		L.offsets.push_back((long long)px);
 		words += d.plane;
 		px += (size_t)d.w * d.h;
@@ -369,6 +374,7 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 				L.bulk.push_back(make_int4((int)f, tx, ty, std::min(ty + rows_per_item, d.h)));
 	}
 	L.total_px = px;
+	L.row_words = (L.row_words + 3) & ~3ll;
 	// Planes padded to 4 words, so every plane starts on a 16-byte boundary.
 	L.plane_words = (words + 3) & ~3ll;
 	L.total_words = (long long)N_PLANES * L.plane_words;
@@ -398,6 +404,7 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	ws.offsets.ensure(nf);
 	if (L.maxiter) {
 		ws.bits.ensure((size_t)L.total_words);
+		ws.rowcand.ensure((size_t)L.row_words);
 		ws.targets.ensure(L.total_px);
 		ws.radius.ensure(L.total_px);
 		ws.cands.ensure(L.total_px);
@@ -408,6 +415,7 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	for (size_t f = 0; f < nf; ++f) {
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
 		L.frames[f].floors = L.maxiter ? ws.floors.p + L.thr_base[f] : nullptr;
+		L.frames[f].rowcand = L.maxiter ? ws.rowcand.p + L.row_off[f] : nullptr;
 	}
 	// Every descriptor array goes through one pinned staging buffer.  The
 	// previous call using this workspace synchronised before returning, so
@@ -487,11 +495,14 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	const int cap = di.sms * L.tune.dense_blocks_per_sm, sparse = di.sms * L.tune.sparse_blocks_per_sm;
 	const int rowb = L.tune.row_blocks_per_sm;
 	{
-		// S1, S2 and CAND of every frame: 3 contiguous planes of 16-byte words.
-		const long long n16 = 3 * L.plane_words / 4;
-		const long long blocks = (n16 + 255) / 256 < di.sms * 4 ? (n16 + 255) / 256 : di.sms * 4;
+		// S1, S2, CAND and FRESH of every frame (4 contiguous planes) and the
+		// row marks, in 16-byte words.
+		const long long n16 = 4 * L.plane_words / 4, m16 = L.row_words / 4;
+		const long long blocks = (n16 + m16 + 255) / 256 < di.sms * 4 ? (n16 + m16 + 255) / 256
+		                                                              : di.sms * 4;
 		zero_words_kernel<<<(int)blocks, 256, 0, s>>>(
-			reinterpret_cast<uint4 *>(ws.bits.p + P_S1 * L.plane_words), n16);
+			reinterpret_cast<uint4 *>(ws.bits.p + P_S1 * L.plane_words), n16,
+			reinterpret_cast<uint4 *>(ws.rowcand.p), m16);
 	}
 	sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
@@ -901,6 +912,7 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 		for (size_t f = 0; f < nf; ++f) {
 			L.frames[f].bits = p->L.frames[f].bits;
 			L.frames[f].floors = p->L.frames[f].floors;
+			L.frames[f].rowcand = p->L.frames[f].rowcand;
 		}
 		p->ims.assign(ims, ims + nf);
 		p->L.frames = L.frames;

@@ -88,13 +88,15 @@ validate_kernel(const double *__restrict__ v, long long n, int minimum, unsigned
 		atomicOr(flags, bit);
 }
 
-// Zero n 16-byte words (the S1, S2 and CAND planes of all frames before a
-// detection pass: they are contiguous in the plane-major layout).
-__global__ void __launch_bounds__(256) zero_words_kernel(uint4 *p, long long n)
+// Zero n 16-byte words at p and m at q (before a detection pass: the S1, S2,
+// CAND and FRESH planes of all frames, contiguous in the plane-major layout,
+// and the row marks).
+__global__ void __launch_bounds__(256) zero_words_kernel(uint4 *p, long long n, uint4 *q,
+	long long m)
 {
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n + m;
 	     i += (long long)gridDim.x * blockDim.x)
-		p[i] = make_uint4(0u, 0u, 0u, 0u);
+		(i < n ? p[i] : q[i - n]) = make_uint4(0u, 0u, 0u, 0u);
 }
 
 __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
@@ -154,6 +156,7 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 	uint32_t *hole_plane = plane_ptr(fd, P_HOLE) + roww, *excl_plane = plane_ptr(fd, P_EXCL) + roww;
 	uint32_t *donor_plane = plane_ptr(fd, P_DONOR) + roww;
 	uint32_t any_hole = 0, any_allowed = 0, any_finite = 0;
+	int ndonor = 0;
 	for (int seg = 0; seg * 1024 < w; ++seg) {
 		uint32_t my_h = 0, my_e = 0, my_d = 0;
 		for (int c0 = 0; c0 < 32; c0 += ROW_UNROLL) {
@@ -198,6 +201,7 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 				any_allowed |= __ballot_sync(0xffffffffu, ok);
 				any_finite |= dw;
 				any_hole |= hw;
+				ndonor += __popc(dw);
 				if (lane == c0 + u) {
 					my_h = hw;
 					my_e = ew;
@@ -219,6 +223,8 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 			set_flag(&st.allowed);
 		if (any_finite)
 			set_flag(&st.finite);
+		if (ndonor)
+			atomicAdd((unsigned long long *)&st.donors_left, (unsigned long long)ndonor);
 	}
 }
 
@@ -267,8 +273,12 @@ __device__ __forceinline__ unsigned long long dilate_row(unsigned long long e)
 
 // Reference src/filters.cuh:177-193 twice (src/cleaner.cuh:123-125) and
 // src/cleaner.cuh:22-37: grown = dilate3x3(dilate3x3(cand) & S1) & S2 on bit
-// planes, fresh = grown & ~crmask, crmask |= grown, per-frame counts of fresh
-// pixels and remaining donors, and fresh pixels appended to the target list.
+// planes, fresh = grown & ~crmask, crmask |= grown, the FRESH plane, the
+// per-frame facts (any fresh pixel; the count of static donors left, which
+// the reference recounts in accumulate), and fresh pixels appended to the
+// target list.  With row marks (fd.rowcand: rows that got a CAND bit this
+// pass) a row without a marked row within two rows is skipped: nothing can
+// grow there, and its FRESH words were zeroed before the pass.
 __global__ void __launch_bounds__(256)
 grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 	const int2 *__restrict__ rows, int nrows, uint2 *targets, Control *ctl)
@@ -281,10 +291,19 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 			continue; // warp-uniform
 		const FrameDesc &fd = frames[item.x];
 		const int w = fd.w, h = fd.h, y = item.y, words = fd.words;
+		// Growth needs a CAND pixel within two rows (two 3 x 3 dilations).
+		if (fd.rowcand) {
+			bool near = false;
+			for (int d = -2; d <= 2; ++d)
+				near |= y + d >= 0 && y + d < h && fd.rowcand[y + d];
+			if (!near)
+				continue; // warp-uniform
+		}
 		const uint32_t *cand = plane_ptr(fd, P_CAND), *s1 = plane_ptr(fd, P_S1);
 		const uint32_t *s2 = plane_ptr(fd, P_S2), *donor = plane_ptr(fd, P_DONOR);
 		uint32_t *crm = plane_ptr(fd, P_CRMASK);
-		uint32_t todo = 0, donors = 0; // any new pixel / any donor left in this row
+		uint32_t todo = 0;
+		int lost = 0; // static donors this row added to the mask
 		for (int k0 = 0; k0 < words; k0 += 32) {
 			const int k = k0 + lane;
 			uint32_t fresh = 0;
@@ -307,7 +326,7 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 					crm[o] = now;
 				plane_ptr(fd, P_FRESH)[o] = fresh;
 				todo |= fresh;
-				donors |= donor[o] & ~now;
+				lost += __popc(fresh & donor[o]);
 			}
 			if (__any_sync(0xffffffffu, fresh != 0)) {
 				unsigned long long slot = warp_append(&ctl->n_targets, __popc(fresh));
@@ -320,12 +339,13 @@ grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 			}
 		}
 		todo = __any_sync(0xffffffffu, todo != 0);
-		donors = __any_sync(0xffffffffu, donors != 0);
+		lost = __reduce_add_sync(0xffffffffu, (unsigned)lost);
 		if (lane == 0) {
 			if (todo)
 				set_flag(&state[item.x].todo);
-			if (donors)
-				set_flag(&state[item.x].donors);
+			if (lost)
+				atomicAdd((unsigned long long *)&state[item.x].donors_left,
+					(unsigned long long)(-(long long)lost));
 		}
 	}
 }
@@ -348,7 +368,7 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 			if (fault) { // this pass's detection is incomplete: stop, report
 				s.fault = 1;
 				s.active = 0;
-			} else if (s.todo && !s.donors) {
+			} else if (s.todo && s.donors_left <= 0) {
 				s.error = 1;
 				s.active = 0;
 			} else if (s.todo) {
@@ -359,7 +379,6 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 			}
 		}
 		s.todo = 0;
-		s.donors = 0;
 		state[f] = s;
 	}
 	any = __syncthreads_or(any);
