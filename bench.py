@@ -229,12 +229,14 @@ def main():
     kinds = _native.KERNEL_KINDS
     kms = {k: sum(p[0][k] for p in prof) / len(prof) for k in kinds}
     klaunch = {k: prof[0][1][k] for k in kinds}
-    # Dense detection kernel (sig_bulk_kernel): per pixel of an active frame it
-    # must read clean (8 B) and clear the S1/S2/CAND bits (3/8 B).  The error
-    # map is not read there: its 32 x 32 block floors are computed once per
-    # call by floor_kernel.
-    active_px = sum(passes) * h * w
-    detect_bytes = active_px * (8 + 3 / 8)
+    # Dense detection kernel (sig_bulk_kernel), run by the first (full) pass
+    # over every frame; its event span also holds the zeroing of the S1, S2,
+    # CAND and FRESH planes before it.  Per pixel: read clean (8 B), zero four
+    # bit planes (4/8 B).  The error map is not read there: its 32 x 32 block
+    # floors are computed once per call by floor_kernel.  Later passes are
+    # incremental and do not run it.
+    active_px = nf * h * w * klaunch["sigraw"]
+    detect_bytes = active_px * (8 + 4 / 8)
     detect_ms = kms["sigraw"]
     achieved = detect_bytes / (detect_ms / 1e3) / 1e9
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
@@ -253,8 +255,8 @@ def main():
                 "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
                 "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
     # Kernels of one execution as the event profiler saw them, plus the plane
-    # zeroing kernel that precedes every dense launch.
-    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"]
+    # zeroing kernel that starts every pass (full or incremental).
+    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"] + klaunch["dirty"]
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),

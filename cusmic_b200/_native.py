@@ -25,7 +25,7 @@ EXPORTS = (
 )
 TUNING_PATH = Path(__file__).with_name("tuning.json")
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
-                "replace", "restore", "copy", "low", "classify", "floor")
+                "replace", "restore", "copy", "low", "classify", "floor", "reclass", "dirty")
 
 
 class Image(ctypes.Structure):

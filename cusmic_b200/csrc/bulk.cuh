@@ -30,9 +30,9 @@
 //  * classify_kernel: sig_raw of each listed pixel, lap / (2 noise), with the
 //    exact noise (error map, or the noise model from the pixel's own 5 x 5
 //    median); above cr_threshold -> high candidate list, else above
-//    neighbor_threshold -> low list (src/filters.cuh:125-135).  The
-//    candidate kernels recompute every value they threshold exactly, so the
-//    lists only have to be supersets.
+//    neighbor_threshold -> low list (src/filters.cuh:125-135), and the same
+//    classes into the HIGH / LOW planes that incremental passes update.  The
+//    candidate kernels recompute every value they threshold exactly.
 //
 // sig_bulk_kernel is warp-specialised.  One producer warp copies clean row
 // segments (BK_COLS columns plus halo columns) into a ring of BK_SLOTS rows in
@@ -770,6 +770,12 @@ classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 						}
 						const double v = pc.lap / (2 * nz);
 						cls = v > prm.cr || v != v ? 1 : v > prm.nb ? 2 : 0;
+					}
+					// The class planes that incremental passes keep up to date.
+					if (cls) {
+						const unsigned px = pix % (unsigned)fd.w, py = pix / (unsigned)fd.w;
+						atomicOr(plane_ptr(fd, cls == 1 ? P_HIGH : P_LOW) +
+							(long long)py * fd.words + (px >> 5), 1u << (px & 31));
 					}
 				}
 				const uint2 entry = make_uint2((unsigned)f, pix);

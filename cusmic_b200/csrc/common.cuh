@@ -33,16 +33,19 @@ enum Plane {
 	P_HOLE,   // non-finite input pixel
 	P_EXCL,   // excluded from seeds and donors: hole or masked
 	P_DONOR,  // static donor: not excluded and finite after background
+	P_CRMASK, // cumulative cosmic-ray mask
+	P_HIGH,   // sig_raw > cr_threshold (or NaN) on the current clean pixels
+	P_LOW,    // neighbor_threshold < sig_raw, not HIGH
 	P_S1,     // significance > cr_threshold
 	P_S2,     // significance > neighbor_threshold
 	P_CAND,   // seed: S1, not excluded, contrast test passed
 	P_FRESH,  // pixels the last growth step added to the mask
-	P_CRMASK, // cumulative cosmic-ray mask
+	P_CHG,    // pixels whose value the last replacement changed
 	N_PLANES
 };
 
 static_assert(P_S2 == P_S1 + 1 && P_CAND == P_S1 + 2 && P_FRESH == P_S1 + 3,
-	"S1, S2, CAND and FRESH are zeroed as one range before each pass");
+	"S1, S2, CAND and FRESH are zeroed as one range before a full pass");
 
 constexpr double FINE_FLOOR = 0.01;   // reference src/filters.cuh:21
 constexpr double SIGNAL_FLOOR = 1e-5; // reference src/filters.cuh:22
@@ -94,7 +97,8 @@ struct FrameDesc {
 	uint8_t *mask_out; // uint8 output mask
 	uint32_t *bits;    // N_PLANES planes of `plane` words
 	BlockFloor *floors; // the frame's block floors, row-major by block (null: none)
-	uint32_t *rowcand;  // per row: nonzero when the row got a CAND bit this pass (null: none)
+	uint32_t *rowcand;  // per row: nonzero when growth must visit the row this pass (null: all)
+	uint32_t *rowchg;   // per row: nonzero when the row has a CHG pixel (null: no tracking)
 	double gain, rn, bg;
 	long long plane;   // words per plane of this frame = h * words
 	long long pstride; // words from one plane to the next (planes of all frames of a
@@ -128,7 +132,7 @@ struct Control {
 	int any_active;
 	int ticket;                   // next item of the bulk detection kernel (reset every pass)
 	int fault;                    // a bounded wait ran out in this pass
-	int pad;
+	int n_dirty;                  // this pass: length of the dirty-row list
 };
 
 CB_HD uint32_t *plane_ptr(const FrameDesc &f, int p)
@@ -140,5 +144,19 @@ CB_HD bool test_bit(const uint32_t *plane, int words, int x, int y)
 {
 	return (plane[(long long)y * words + (x >> 5)] >> (x & 31)) & 1u;
 }
+
+#ifdef __CUDACC__
+// Sets or clears bit `bit` of *word, for a caller that is the only writer of
+// that bit (other bits of the word may change concurrently): an atomic only
+// when the bit changes.
+__device__ __forceinline__ void write_bit(uint32_t *word, uint32_t bit, bool value)
+{
+	const bool now = (*(volatile uint32_t *)word & bit) != 0;
+	if (value && !now)
+		atomicOr(word, bit);
+	else if (!value && now)
+		atomicAnd(word, ~bit);
+}
+#endif
 
 } // namespace cb

@@ -485,12 +485,13 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 	}
 	const double sig = center - med;
 	if (lane == 0) {
+		// Set or clear: an incremental pass keeps the bits of the previous
+		// pass and re-evaluates some pixels.
 		const long long word = (long long)y * fd.words + (x >> 5);
 		const uint32_t bit = 1u << (x & 31);
-		if (sig > prm.nb)
-			atomicOr(plane_ptr(fd, P_S2) + word, bit);
-		if (!LOW && sig > prm.cr)
-			atomicOr(plane_ptr(fd, P_S1) + word, bit);
+		write_bit(plane_ptr(fd, P_S2) + word, bit, sig > prm.nb);
+		if (!LOW)
+			write_bit(plane_ptr(fd, P_S1) + word, bit, sig > prm.cr);
 	}
 	nz_center_out = nz_center;
 	return sig;
@@ -505,8 +506,11 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 	const double sig = candidate_sig<LOW>(fd, x, y, P, prm, nz);
 	if (!LOW && (threadIdx.x & 31) == 0) {
 		const long long word = (long long)y * fd.words + (x >> 5);
-		const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & (1u << (x & 31)));
+		const uint32_t bit = 1u << (x & 31);
+		const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
 		seeds[e] = seed ? Seed{t.x, t.y, sig, nz} : Seed{NO_SEED, 0, 0.0, 0.0};
+		if (!seed) // the seed kernel decides the CAND bit of a seed
+			write_bit(plane_ptr(fd, P_CAND) + word, bit, false);
 	}
 }
 
@@ -665,15 +669,14 @@ __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, dou
 	}
 	const double med3c = __shfl_sync(0xffffffffu, m3[0], 24);
 	const double med7 = warp_rank64(m3[0], m3[1], 24);
-	if (lane == 0) {
-		double fine = (med3c - med7) / noise;
-		fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
-		if (sig / fine > prm.contrast) {
-			atomicOr(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
-			if (fd.rowcand)
-				fd.rowcand[y] = 1u;
-		}
-	}
+	double fine = (med3c - med7) / noise;
+	fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
+	const bool cand = sig / fine > prm.contrast;
+	if (lane == 0)
+		write_bit(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31), cand);
+	// Growth can flag pixels within two rows of a CAND pixel.
+	if (cand && fd.rowcand && lane < 5 && y + lane - 2 >= 0 && y + lane - 2 < h)
+		fd.rowcand[y + lane - 2] = 1u;
 }
 
 // C (list-based): one warp per seed slot.

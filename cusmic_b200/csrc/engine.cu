@@ -13,6 +13,7 @@
 #include "detect.cuh"
 #include "bulk.cuh"
 #include "kernels.cuh"
+#include "incremental.cuh"
 #include "backward.cuh"
 
 #include <algorithm>
@@ -132,6 +133,7 @@ struct Layout {
 	size_t total_px = 0;
 	DetectParams prm{};
 	int maxiter = 0;
+	int error_frames = 0; // frames with an error map (a rebound plan keeps which)
 	cusmic_tuning tune{};
 };
 
@@ -158,9 +160,10 @@ struct Workspace {
 	DevBuf<FrameState> state;
 	DevBuf<int2> rows;
 	DevBuf<uint32_t> bits;
-	DevBuf<uint32_t> rowcand;
+	DevBuf<uint32_t> rowmarks; // growth row marks, then CHG row marks (row_words each)
 	DevBuf<uint2> targets;
 	DevBuf<uint8_t> radius; // per target: window radius of its last replacement
+	DevBuf<int2> dirty;     // dirty-row list of an incremental pass
 	DevBuf<uint2> cands;
 	DevBuf<Seed> seeds;
 	DevBuf<int4> bulk;
@@ -327,6 +330,7 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		FrameScalars s = scalars_for(o, sc, f);
 		d.data = im.data;
 		d.error = im.error;
+		L.error_frames += im.error != nullptr;
 		d.gain_map = im.error ? nullptr : im.gain;
 		d.rn_map = im.error ? nullptr : im.readnoise;
 		d.bg_map = im.background;
@@ -404,9 +408,10 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	ws.offsets.ensure(nf);
 	if (L.maxiter) {
 		ws.bits.ensure((size_t)L.total_words);
-		ws.rowcand.ensure((size_t)L.row_words);
+		ws.rowmarks.ensure(2 * (size_t)L.row_words);
 		ws.targets.ensure(L.total_px);
 		ws.radius.ensure(L.total_px);
+		ws.dirty.ensure(L.rows.size());
 		ws.cands.ensure(L.total_px);
 		ws.seeds.ensure(L.total_px);
 		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
@@ -415,7 +420,8 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	for (size_t f = 0; f < nf; ++f) {
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
 		L.frames[f].floors = L.maxiter ? ws.floors.p + L.thr_base[f] : nullptr;
-		L.frames[f].rowcand = L.maxiter ? ws.rowcand.p + L.row_off[f] : nullptr;
+		L.frames[f].rowcand = L.maxiter ? ws.rowmarks.p + L.row_off[f] : nullptr;
+		L.frames[f].rowchg = L.maxiter ? ws.rowmarks.p + L.row_words + L.row_off[f] : nullptr;
 	}
 	// Every descriptor array goes through one pinned staging buffer.  The
 	// previous call using this workspace synchronised before returning, so
@@ -453,7 +459,7 @@ struct GraphLoop {
 
 // Kernel kinds reported by cusmic_plan_profile().
 enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_SIGRAW, K_CAND, K_SEED, K_GROW, K_CONTROL,
-	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_CLASSIFY, K_FLOOR, K_KINDS };
+	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_CLASSIFY, K_FLOOR, K_RECLASS, K_DIRTY, K_KINDS };
 
 // Optional CUDA-event timer: an event after every launch on the launching
 // stream, so each kernel's duration is the gap to the previous event.
@@ -487,30 +493,51 @@ static inline void mark(Recorder *r, int kind)
 		r->mark(kind);
 }
 
+// One detection pass.  The first pass of a call is full: the dense kernel
+// lists every candidate and the classification fills the HIGH / LOW planes.
+// Later passes are incremental (incremental.cuh): they start from the pixels
+// that the last replacement changed and keep the other bits.
 static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
-	const GraphLoop &gl, Recorder *rec = nullptr)
+	const GraphLoop &gl, bool incremental, Recorder *rec = nullptr)
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
 	const int nbulk = (int)L.bulk.size();
 	const int cap = di.sms * L.tune.dense_blocks_per_sm, sparse = di.sms * L.tune.sparse_blocks_per_sm;
 	const int rowb = L.tune.row_blocks_per_sm;
 	{
-		// S1, S2, CAND and FRESH of every frame (4 contiguous planes) and the
-		// row marks, in 16-byte words.
-		const long long n16 = 4 * L.plane_words / 4, m16 = L.row_words / 4;
+		// Full: S1, S2, CAND and FRESH of every frame (contiguous planes) and
+		// the growth row marks; incremental: FRESH (its growth visits a row
+		// list).  In 16-byte words.
+		const int first = incremental ? P_FRESH : P_S1, planes = incremental ? 1 : 4;
+		const long long n16 = planes * L.plane_words / 4, m16 = incremental ? 0 : L.row_words / 4;
 		const long long blocks = (n16 + m16 + 255) / 256 < di.sms * 4 ? (n16 + m16 + 255) / 256
 		                                                              : di.sms * 4;
 		zero_words_kernel<<<(int)blocks, 256, 0, s>>>(
-			reinterpret_cast<uint4 *>(ws.bits.p + P_S1 * L.plane_words), n16,
-			reinterpret_cast<uint4 *>(ws.rowcand.p), m16);
+			reinterpret_cast<uint4 *>(ws.bits.p + first * L.plane_words), n16,
+			reinterpret_cast<uint4 *>(ws.rowmarks.p), m16);
 	}
-	sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
-		ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
-	mark(rec, K_SIGRAW);
-	const int cgrid = (nbulk * BK_CWARPS + 7) / 8 < sparse ? (nbulk * BK_CWARPS + 7) / 8 : sparse;
-	classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
-		ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
-	mark(rec, K_CLASSIFY);
+	if (incremental) {
+		const int tb = (nrows + 255) / 256 < di.sms * 4 ? (nrows + 255) / 256 : di.sms * 4;
+		dirty_rows_kernel<<<tb, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows, L.prm.mode,
+			ws.ctl.p, ws.dirty.p);
+		mark(rec, K_DIRTY);
+		const int rgrid = grid_for_rows(di, nrows, rowb);
+		if (L.error_frames)
+			incremental_rows_kernel<false><<<rgrid, 256, 0, s>>>(ws.frames.p, ws.dirty.p,
+				&ws.ctl.p->n_dirty, L.prm, ws.ctl.p, ws.cands.p);
+		if (L.error_frames < nf)
+			incremental_rows_kernel<true><<<rgrid, 256, 0, s>>>(ws.frames.p, ws.dirty.p,
+				&ws.ctl.p->n_dirty, L.prm, ws.ctl.p, ws.cands.p);
+		mark(rec, K_RECLASS);
+	} else {
+		sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
+		mark(rec, K_SIGRAW);
+		const int cgrid = (nbulk * BK_CWARPS + 7) / 8 < sparse ? (nbulk * BK_CWARPS + 7) / 8 : sparse;
+		classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
+			ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
+		mark(rec, K_CLASSIFY);
+	}
 	candidate_high_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
 		ws.seeds.p);
 	mark(rec, K_CAND);
@@ -518,8 +545,10 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	mark(rec, K_SEED);
 	candidate_low_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p);
 	mark(rec, K_LOW);
+	// An incremental pass grows on its dirty rows only.
 	grow_update_kernel<<<grid_for_rows(di, nrows, rowb), 256, 0, s>>>(ws.frames.p, ws.state.p,
-		ws.rows.p, nrows, ws.targets.p, ws.ctl.p);
+		incremental ? ws.dirty.p : ws.rows.p, nrows, incremental ? &ws.ctl.p->n_dirty : nullptr,
+		ws.targets.p, ws.ctl.p);
 	mark(rec, K_GROW);
 	control_kernel<<<1, 1024, 0, s>>>(ws.state.p, nf, ws.ctl.p, gl.handle, gl.use ? 1 : 0);
 	mark(rec, K_CONTROL);
@@ -540,8 +569,9 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		mark(rec, K_COPY);
 		return;
 	}
-	// Zero bit planes: prepare_kernel writes HOLE, EXCL and DONOR.
+	// Zero bit planes (prepare_kernel writes HOLE, EXCL and DONOR) and row marks.
 	check(cudaMemsetAsync(ws.bits.p, 0, (size_t)L.total_words * sizeof(uint32_t), s));
+	check(cudaMemsetAsync(ws.rowmarks.p, 0, 2 * (size_t)L.row_words * sizeof(uint32_t), s));
 	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
 		nrows);
 	mark(rec, K_PREPARE);
@@ -575,7 +605,7 @@ static void enqueue_plain(Workspace &ws, const Layout &L, const DeviceInfo &di, 
 		rec->begin(s);
 	launch_prologue(ws, L, di, s, rec);
 	for (int it = 0; it < L.maxiter; ++it)
-		launch_pass(ws, L, di, s, GraphLoop{}, rec);
+		launch_pass(ws, L, di, s, GraphLoop{}, it > 0, rec);
 	launch_epilogue(ws, L, di, s, rec);
 	check(cudaGetLastError());
 }
@@ -816,8 +846,13 @@ static void capture_graph(cusmic_plan &p)
 			const cudaGraphNode_t *deps = nullptr;
 			size_t nd = 0;
 			check(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
+			// The full first pass sets the loop condition (its control
+			// kernel runs upstream of the while node); the body repeats the
+			// incremental pass.
 			cudaGraphConditionalHandle handle;
-			check(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+			check(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+			launch_pass(p.ws, p.L, p.di, cs, GraphLoop{handle, true}, false);
+			check(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
 			cudaGraphNodeParams cp = {};
 			cp.type = cudaGraphNodeTypeConditional;
 			cp.conditional.handle = handle;
@@ -833,7 +868,7 @@ static void capture_graph(cusmic_plan &p)
 			cudaError_t err = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
 				cudaStreamCaptureModeThreadLocal);
 			if (err == cudaSuccess) {
-				launch_pass(p.ws, p.L, p.di, bs, GraphLoop{handle, true});
+				launch_pass(p.ws, p.L, p.di, bs, GraphLoop{handle, true}, true);
 				err = cudaStreamEndCapture(bs, nullptr);
 			}
 			cudaStreamDestroy(bs);
@@ -913,6 +948,7 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 			L.frames[f].bits = p->L.frames[f].bits;
 			L.frames[f].floors = p->L.frames[f].floors;
 			L.frames[f].rowcand = p->L.frames[f].rowcand;
+			L.frames[f].rowchg = p->L.frames[f].rowchg;
 		}
 		p->ims.assign(ims, ims + nf);
 		p->L.frames = L.frames;
@@ -1262,7 +1298,8 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 				candidate_high_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
 				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl);
 				candidate_low_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl);
-				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, targets, ctl);
+				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, nullptr, targets,
+					ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
 				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, nullptr);
 			}

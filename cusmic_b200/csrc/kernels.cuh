@@ -276,28 +276,36 @@ __device__ __forceinline__ unsigned long long dilate_row(unsigned long long e)
 // planes, fresh = grown & ~crmask, crmask |= grown, the FRESH plane, the
 // per-frame facts (any fresh pixel; the count of static donors left, which
 // the reference recounts in accumulate), and fresh pixels appended to the
-// target list.  With row marks (fd.rowcand: rows that got a CAND bit this
-// pass) a row without a marked row within two rows is skipped: nothing can
-// grow there, and its FRESH words were zeroed before the pass.
+// target list.  The row list holds nrows rows, or *dev_nrows when that is
+// not null.  With row marks (fd.rowcand) an unmarked row is skipped: nothing
+// can grow there, and its FRESH words were zeroed before the pass.  A full
+// pass marks the rows within two of a CAND pixel (two 3 x 3 dilations); an
+// incremental pass lists the rows within six of a pixel whose value the last
+// replacement changed, and marks them.  A visited row's CHG bits and mark are
+// cleared (every row with a CHG bit is visited).
 __global__ void __launch_bounds__(256)
 grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
-	const int2 *__restrict__ rows, int nrows, uint2 *targets, Control *ctl)
+	const int2 *__restrict__ rows, int nrows, const int *dev_nrows, uint2 *targets, Control *ctl)
 {
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+	if (dev_nrows)
+		nrows = *dev_nrows;
 	for (int r = gw; r < nrows; r += nw) {
 		const int2 item = rows[r];
 		if (!state[item.x].active)
 			continue; // warp-uniform
 		const FrameDesc &fd = frames[item.x];
 		const int w = fd.w, h = fd.h, y = item.y, words = fd.words;
-		// Growth needs a CAND pixel within two rows (two 3 x 3 dilations).
-		if (fd.rowcand) {
-			bool near = false;
-			for (int d = -2; d <= 2; ++d)
-				near |= y + d >= 0 && y + d < h && fd.rowcand[y + d];
-			if (!near)
-				continue; // warp-uniform
+		if (fd.rowcand && !fd.rowcand[y])
+			continue; // warp-uniform: no pixel of the row can be flagged this pass
+		if (fd.rowchg && fd.rowchg[y]) {
+			// The pass has read the row's CHG bits: clear them for the
+			// replacement that follows.
+			for (int k = lane; k < words; k += 32)
+				plane_ptr(fd, P_CHG)[(long long)y * words + k] = 0u;
+			if (lane == 0)
+				fd.rowchg[y] = 0u;
 		}
 		const uint32_t *cand = plane_ptr(fd, P_CAND), *s1 = plane_ptr(fd, P_S1);
 		const uint32_t *s2 = plane_ptr(fd, P_S2), *donor = plane_ptr(fd, P_DONOR);
@@ -388,6 +396,7 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 		ctl->n_cand = 0;
 		ctl->n_low = 0;
 		ctl->ticket = 0;
+		ctl->n_dirty = 0;
 		if (use_handle)
 			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
 	}
@@ -492,7 +501,7 @@ __device__ double select_rank(const FrameDesc &fd, const uint32_t *don, const ui
 // Reference src/replace.cuh:111-153 for one pixel, by the whole warp: the
 // median of the donors in the clipped (2r+1)^2 window, r = 2, 3, ... until a
 // donor exists; lane 0 writes it.  Returns r (0: the frame has no donor).
-__device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y)
+__device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y, bool *changed = nullptr)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, words = fd.words;
@@ -530,7 +539,10 @@ __device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y)
 		}
 		if (lane == 0) {
 			const double v = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
-			fd.clean[(long long)y * w + x] = v;
+			double &dst = fd.clean[(long long)y * w + x];
+			if (changed)
+				*changed = __double_as_longlong(dst) != __double_as_longlong(v);
+			dst = v;
 			// Keep the block's floor a lower bound of its clean values.
 			if (fd.floors && !fd.error)
 				atomicMin(&fd.floors[(y >> 5) * ((w + 31) >> 5) + (x >> 5)].key, order_key(v));
@@ -548,6 +560,9 @@ __device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y)
 // growth step flagged no pixel keeps its value: its donors (static donors not
 // in the mask) and their values are unchanged, so the same window and the
 // same median would come out.
+//
+// With fd.rowchg, a target whose value changed (bit for bit) gets its CHG
+// bit and its row mark: the next incremental pass starts from those pixels.
 __global__ void __launch_bounds__(256)
 replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const uint2 *__restrict__ list, const unsigned long long *count, uint8_t *radius)
@@ -558,22 +573,32 @@ replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restric
 	const long long n = (long long)*count;
 	for (long long e = gw; e < n; e += nw) {
 		const uint2 t = list[e];
-		if (!state[t.x].replace)
-			continue;
-		const FrameDesc &fd = frames[t.x];
-		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
-		if (radius && radius[e] == 2) {
-			const uint32_t *fr = plane_ptr(fd, P_FRESH);
-			unsigned long long any = 0;
+		if (state[t.x].replace) { // warp-uniform
+			bool ch = false;
+			const FrameDesc &fd = frames[t.x];
+			const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+			bool keep = false;
+			if (radius && radius[e] == 2) {
+				const uint32_t *fr = plane_ptr(fd, P_FRESH);
+				unsigned long long any = 0;
 #pragma unroll
-			for (int d = -2; d <= 2; ++d)
-				any |= bit_window(fr, fd.words, fd.h, y + d, x >> 5);
-			if (!((any >> (x & 31)) & 0x1full))
-				continue; // warp-uniform
+				for (int d = -2; d <= 2; ++d)
+					any |= bit_window(fr, fd.words, fd.h, y + d, x >> 5);
+				keep = !((any >> (x & 31)) & 0x1full);
+			}
+			if (!keep) { // warp-uniform
+				const int r = replace_one(fd, x, y, &ch);
+				if (lane == 0) {
+					if (radius)
+						radius[e] = (uint8_t)(r < 255 ? r : 255);
+					if (ch && fd.rowchg) {
+						atomicOr(plane_ptr(fd, P_CHG) + (long long)y * fd.words + (x >> 5),
+							1u << (x & 31));
+						fd.rowchg[y] = 1u;
+					}
+				}
+			}
 		}
-		const int r = replace_one(fd, x, y);
-		if (radius && lane == 0)
-			radius[e] = (uint8_t)(r < 255 ? r : 255);
 	}
 }
 

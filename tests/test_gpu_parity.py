@@ -390,3 +390,53 @@ def test_host_api_map_contents(cuda, maps, message):
                                       mask.ctypes.data, msg, 128)
     assert st == _native.CUSMIC_INVALID and msg.value.decode() == message
     assert (clean == 9).all() and (mask == 9).all()
+
+
+def clustered_scene(seed, h, w):
+    """Cosmic-ray clusters whose halos fall off gradually, so a low
+    neighbor_threshold keeps flagging pixels next to the last pass's
+    replacements for several passes."""
+    rng = np.random.default_rng(seed)
+    data = 200 + rng.normal(0, 15, (h, w))
+    for _ in range(max(1, h * w // 60)):
+        y, x = int(rng.integers(0, h)), int(rng.integers(0, w))
+        amp = rng.uniform(500, 20000)
+        for dy in range(-3, 4):
+            for dx in range(-3, 4):
+                if 0 <= y + dy < h and 0 <= x + dx < w:
+                    data[y + dy, x + dx] += amp * rng.uniform(0.05, 0.7) ** (abs(dy) + abs(dx))
+    return data
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("path", ("error", "model"))
+@pytest.mark.parametrize("shape", ((7, 9), (12, 13), (26, 30), (90, 77)))
+def test_incremental_passes(cuda, oracle, mode, path, shape):
+    """Passes after the first re-evaluate only the neighbourhood of the pixels
+    the last replacement changed: many passes (maxiter 8), frames narrower
+    than that neighbourhood (wrap folds it onto itself), every border mode."""
+    h, w = shape
+    seed = h * 1000 + w * 10 + MODES.index(mode) * 2 + (path == "model")
+    data = clustered_scene(seed, h, w)
+    frame = dict(data=data)
+    opts = dict(contrast=1.0, cr_threshold=4.0, neighbor_threshold=1.5, maxiter=8, border=mode)
+    if path == "error":
+        frame["error"] = np.sqrt(np.abs(data) / 1.5 + 16)
+    else:
+        frame.update(gain=1.5, readnoise=4.0)
+        opts.update(gain=1.5, readnoise=4.0)
+    settings = {k: v for k, v in opts.items() if k not in ("gain", "readnoise")}
+    _, _, passes = cabi.oracle_frame(oracle, frame, **settings)
+    if h * w > 1000:
+        assert passes >= 3  # the scene exercises the incremental passes
+    check_against_oracle(oracle, [frame], opts)
+
+
+def test_incremental_passes_ragged_stops(cuda, oracle):
+    """A ragged batch whose frames stop after different numbers of passes."""
+    frames = []
+    for i, (h, w) in enumerate(((60, 70), (33, 130), (9, 7), (80, 41), (20, 200))):
+        data = clustered_scene(500 + i, h, w) if i % 2 == 0 else small_scene(500 + i, h, w)[0]
+        frames.append(dict(data=data, error=np.sqrt(np.abs(data) / 1.5 + 16)))
+    check_against_oracle(oracle, frames, dict(contrast=1.0, cr_threshold=4.0,
+                                              neighbor_threshold=1.5, maxiter=6), ragged=True)
