@@ -49,6 +49,35 @@ namespace cb {
 
 static_assert(FLOOR_BLOCK == 32, "a bit word of a row lies in one floor block");
 
+// model_threshold of block (bx, by) of a noise-model frame; outside wrap mode
+// only the 3 x 3 neighbouring blocks count, read directly.
+__device__ __forceinline__ double block_threshold(const FrameDesc &fd, int bx, int by, int mode,
+	double tmin2)
+{
+	if (mode == WRAP)
+		return model_threshold(fd, bx, by, mode, tmin2);
+	const BlockFloor *bf = fd.floors;
+	const int bw = (fd.w + FLOOR_BLOCK - 1) / FLOOR_BLOCK, bh = (fd.h + FLOOR_BLOCK - 1) / FLOOR_BLOCK;
+	unsigned long long key = ~0ull;
+#pragma unroll
+	for (int i = -1; i <= 1; ++i)
+#pragma unroll
+		for (int j = -1; j <= 1; ++j) {
+			const int yy = by + i, xx = bx + j;
+			if (yy >= 0 && yy < bh && xx >= 0 && xx < bw)
+				key = min(key, bf[yy * bw + xx].key);
+		}
+	if (mode == CONSTANT && (bx == 0 || by == 0 || (bx + 1) * FLOOR_BLOCK + 2 > fd.w ||
+		(by + 1) * FLOOR_BLOCK + 2 > fd.h))
+		key = min(key, order_key(0.0));
+	double m = order_value(key);
+	m = m < SIGNAL_FLOOR ? SIGNAL_FLOOR : m;
+	const BlockFloor &own = bf[by * bw + bx];
+	const double g = fd.gain_map ? -order_value(own.gkey) : fd.gain;
+	const double rn = fd.rn_map ? order_value(own.rkey) : fd.rn;
+	return tmin2 * (sqrt(rn * rn + g * m) / g);
+}
+
 // The Laplacian at an in-frame pixel (reference src/filters.cuh:98-104).
 __device__ __forceinline__ double lap_at(const FrameDesc &fd, int x, int y, int lm)
 {
@@ -231,7 +260,7 @@ __device__ __forceinline__ NearMasks near_changed(const FrameDesc &fd, int y, in
 //    within 6 to the low list (back).
 // A row's classes are all this needs from the pass, so no other row waits.
 template <bool MODEL>
-__global__ void __launch_bounds__(256, MODEL ? 2 : 3)
+__global__ void __launch_bounds__(256, 3)
 incremental_rows_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ rows,
 	const int *nrows, DetectParams prm, Control *ctl, uint2 *cands)
 {
@@ -309,7 +338,7 @@ incremental_rows_kernel(const FrameDesc *__restrict__ frames, const int2 *__rest
 					// kernel's superset test): lap <= T gives sig_raw below both
 					// thresholds without the pixel's 5 x 5 median.  The pixels
 					// that pass are compacted to the front of the queue.
-					thr[warp][lane] = nm.r2 ? model_threshold(fd, k, y / FLOOR_BLOCK, mode, tmin2) : 0.0;
+					thr[warp][lane] = nm.r2 ? block_threshold(fd, k, y / FLOOR_BLOCK, mode, tmin2) : 0.0;
 					__syncwarp();
 					todo = 0;
 					for (int q0 = 0; q0 < total; q0 += 32) {
@@ -329,32 +358,41 @@ incremental_rows_kernel(const FrameDesc *__restrict__ frames, const int2 *__rest
 					}
 				}
 				__syncwarp();
-				for (int q0 = 0; q0 < todo; q0 += 32) {
-					if (q0 + lane < todo) {
-						const int e = Q[q0 + lane], kk = e >> 5, bit = e & 31;
+				if (MODEL) {
+					// Exact sig_raw of each pixel that passed, one at a time: its
+					// 5 x 5 window of clean one cell per lane, sorted across the
+					// warp (+inf padding), the median at rank 12.
+					for (int q = 0; q < todo; ++q) {
+						const int e = Q[q], kk = e >> 5, bit = e & 31;
 						const int px = 32 * (k0 + kk) + bit;
-						const long long i = (long long)y * w + px;
-						const double lap = lap_at(fd, px, y, lm);
-						double nz;
-						if (!MODEL) {
-							nz = fd.error[i];
-						} else if (px >= 2 && y >= 2 && px + 2 < w && y + 2 < fd.h) {
-							double win[25];
-							const double *src = fd.clean + i - 2 * (long long)w - 2;
-#pragma unroll
-							for (int a = 0; a < 5; ++a)
-#pragma unroll
-								for (int c = 0; c < 5; ++c)
-									win[a * 5 + c] = src[(long long)a * w + c];
-							nz = noise_from_median(fd, i, median_network(win));
-						} else {
-							nz = noise_model_at(fd, px, y, mode);
+						double c = INFINITY;
+						if (lane < 25) {
+							const int cx = px + lane % 5 - 2, cy = y + lane / 5 - 2;
+							c = cx >= 0 && cy >= 0 && cx < w && cy < fd.h
+								? fd.clean[(long long)cy * w + cx] : clean_at(fd, cx, cy, mode);
 						}
-						const double v = lap / (2 * nz);
-						if (v > prm.cr || v != v)
-							atomicOr(&hmask[warp][kk], 1u << bit);
-						else if (v > prm.nb)
-							atomicOr(&lmask[warp][kk], 1u << bit);
+						const double m = __shfl_sync(0xffffffffu, warp_sort32(c), 12);
+						if (lane == 0) {
+							const long long i = (long long)y * w + px;
+							const double v = lap_at(fd, px, y, lm) / (2 * noise_from_median(fd, i, m));
+							if (v > prm.cr || v != v)
+								hmask[warp][kk] |= 1u << bit;
+							else if (v > prm.nb)
+								lmask[warp][kk] |= 1u << bit;
+						}
+					}
+				} else {
+					for (int q0 = 0; q0 < todo; q0 += 32) {
+						if (q0 + lane < todo) {
+							const int e = Q[q0 + lane], kk = e >> 5, bit = e & 31;
+							const int px = 32 * (k0 + kk) + bit;
+							const long long i = (long long)y * w + px;
+							const double v = lap_at(fd, px, y, lm) / (2 * fd.error[i]);
+							if (v > prm.cr || v != v)
+								atomicOr(&hmask[warp][kk], 1u << bit);
+							else if (v > prm.nb)
+								atomicOr(&lmask[warp][kk], 1u << bit);
+						}
 					}
 				}
 				__syncwarp();
