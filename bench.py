@@ -254,9 +254,10 @@ def main():
                 "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4),
                 "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
                 "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
-    # Kernels of one execution as the event profiler saw them, plus the plane
-    # zeroing kernel that starts every pass (full or incremental).
-    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"] + klaunch["dirty"]
+    # Kernels of one execution as the event profiler saw them, plus two per
+    # pass that share a mark with another kernel: the plane zeroing that starts
+    # every pass (full or incremental) and the replacement's target selection.
+    launches_per_step = sum(klaunch.values()) + 2 * (klaunch["sigraw"] + klaunch["dirty"])
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),

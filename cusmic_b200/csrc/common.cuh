@@ -133,6 +133,8 @@ struct Control {
 	int ticket;                   // next item of the bulk detection kernel (reset every pass)
 	int fault;                    // a bounded wait ran out in this pass
 	int n_dirty;                  // this pass: length of the dirty-row list
+	unsigned n_sel;               // this pass: targets the replacement visits
+	unsigned pad;
 };
 
 CB_HD uint32_t *plane_ptr(const FrameDesc &f, int p)

@@ -164,6 +164,7 @@ struct Workspace {
 	DevBuf<uint2> targets;
 	DevBuf<uint8_t> radius; // per target: window radius of its last replacement
 	DevBuf<int2> dirty;     // dirty-row list of an incremental pass
+	DevBuf<unsigned> sel;   // targets the replacement after a pass visits
 	DevBuf<uint2> cands;
 	DevBuf<Seed> seeds;
 	DevBuf<int4> bulk;
@@ -412,6 +413,7 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 		ws.targets.ensure(L.total_px);
 		ws.radius.ensure(L.total_px);
 		ws.dirty.ensure(L.rows.size());
+		ws.sel.ensure(L.total_px);
 		ws.cands.ensure(L.total_px);
 		ws.seeds.ensure(L.total_px);
 		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
@@ -552,8 +554,11 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	mark(rec, K_GROW);
 	control_kernel<<<1, 1024, 0, s>>>(ws.state.p, nf, ws.ctl.p, gl.handle, gl.use ? 1 : 0);
 	mark(rec, K_CONTROL);
+	const int tb = di.sms * 4;
+	replace_select_kernel<<<tb, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
+		&ws.ctl.p->n_targets, ws.radius.p, ws.ctl.p, ws.sel.p);
 	replace_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
-		&ws.ctl.p->n_targets, ws.radius.p);
+		&ws.ctl.p->n_targets, ws.sel.p, &ws.ctl.p->n_sel, ws.radius.p);
 	mark(rec, K_REPLACE);
 }
 
@@ -1301,7 +1306,8 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, nullptr, targets,
 					ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
-				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, nullptr);
+				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, nullptr,
+					nullptr, nullptr);
 			}
 			restore_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
 		}

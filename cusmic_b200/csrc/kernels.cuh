@@ -397,6 +397,7 @@ control_kernel(FrameState *state, int nf, Control *ctl, cudaGraphConditionalHand
 		ctl->n_low = 0;
 		ctl->ticket = 0;
 		ctl->n_dirty = 0;
+		ctl->n_sel = 0;
 		if (use_handle)
 			cudaGraphSetConditional(handle, (any && it < ctl->maxiter) ? 1u : 0u);
 	}
@@ -552,51 +553,102 @@ __device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y, bo
 	return 0;
 }
 
-// Replacement of the target list after a pass, one warp per target, for
-// frames whose pass flagged new pixels.
+// Largest window radius whose FRESH neighbourhood replace_kernel inspects.
+constexpr int KEEP_RADIUS_MAX = 15;
+
+// Any FRESH pixel in the (2r + 1)^2 window of (x, y) clipped to the frame
+// (r <= KEEP_RADIUS_MAX: a window row spans at most two bit words).
+__device__ __forceinline__ bool fresh_in_window(const FrameDesc &fd, int x, int y, int r)
+{
+	const uint32_t *fr = plane_ptr(fd, P_FRESH);
+	const int x0 = max(0, x - r), x1 = min(fd.w - 1, x + r);
+	const int k0 = x0 >> 5, k1 = x1 >> 5;
+	const unsigned long long span = ((1ull << (x1 - x0 + 1)) - 1ull) << (x0 & 31);
+	const int ya = max(0, y - r), yb = min(fd.h - 1, y + r);
+	const uint32_t *c0 = fr + (long long)ya * fd.words + k0;
+	const int dk = k1 - k0; // 0 or 1
+	unsigned long long any = 0;
+#pragma unroll 4
+	for (int i = 0; i <= yb - ya; ++i) { // independent loads, no early exit
+		const uint32_t *c = c0 + (long long)i * fd.words;
+		any |= (c[0] | (unsigned long long)c[dk] << 32) & span;
+	}
+	return any != 0;
+}
+
+// Which targets the replacement after a pass must visit, for frames whose
+// pass flagged new pixels: a lane per target; the indices of those to visit
+// are appended to `sel` (count in ctl->n_sel).
 //
-// radius (may be null) keeps, per target, the window radius of its last
-// replacement.  A target whose last window had radius 2 and in which the last
-// growth step flagged no pixel keeps its value: its donors (static donors not
-// in the mask) and their values are unchanged, so the same window and the
-// same median would come out.
+// radius keeps, per target, the window radius of its last replacement.  A
+// target whose last window (radius r <= KEEP_RADIUS_MAX) holds no pixel the
+// last growth step flagged keeps its value: donors are never added (the mask
+// only grows) and keep their values, so the smaller windows still hold none,
+// the same window holds the same donors, and the same median would come out.
+// A new target is itself a flagged pixel.
+__global__ void __launch_bounds__(256)
+replace_select_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
+	const uint2 *__restrict__ list, const unsigned long long *count,
+	const uint8_t *__restrict__ radius, Control *ctl, unsigned *sel)
+{
+	const int lane = threadIdx.x & 31;
+	const long long n = (long long)*count;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+	     base += stride) {
+		const long long e = base + lane;
+		bool todo = false;
+		if (e < n) {
+			const uint2 t = list[e];
+			if (state[t.x].replace) {
+				todo = true;
+				const int r = radius[e];
+				if (r <= KEEP_RADIUS_MAX) {
+					const FrameDesc &fd = frames[t.x];
+					todo = fresh_in_window(fd, (int)(t.y % (unsigned)fd.w), (int)(t.y / (unsigned)fd.w), r);
+				}
+			}
+		}
+		const unsigned b = __ballot_sync(0xffffffffu, todo);
+		unsigned at = 0;
+		if (lane == 0 && b)
+			at = atomicAdd(&ctl->n_sel, (unsigned)__popc(b));
+		at = __shfl_sync(0xffffffffu, at, 0);
+		if (todo)
+			sel[at + __popc(b & ((1u << lane) - 1u))] = (unsigned)e;
+	}
+}
+
+// Replacement after a pass, one warp per target: the targets listed in sel
+// (with radius: each replacement's window radius is kept), or with sel null
+// every target of the frames whose pass flagged new pixels.
 //
 // With fd.rowchg, a target whose value changed (bit for bit) gets its CHG
 // bit and its row mark: the next incremental pass starts from those pixels.
 __global__ void __launch_bounds__(256)
 replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
-	const uint2 *__restrict__ list, const unsigned long long *count, uint8_t *radius)
+	const uint2 *__restrict__ list, const unsigned long long *count, const unsigned *sel,
+	const unsigned *nsel, uint8_t *radius)
 {
 	const int lane = threadIdx.x & 31;
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-	const long long n = (long long)*count;
-	for (long long e = gw; e < n; e += nw) {
+	const long long n = sel ? (long long)*nsel : (long long)*count;
+	for (long long s = gw; s < n; s += nw) {
+		const long long e = sel ? (long long)sel[s] : s;
 		const uint2 t = list[e];
-		if (state[t.x].replace) { // warp-uniform
-			bool ch = false;
-			const FrameDesc &fd = frames[t.x];
-			const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
-			bool keep = false;
-			if (radius && radius[e] == 2) {
-				const uint32_t *fr = plane_ptr(fd, P_FRESH);
-				unsigned long long any = 0;
-#pragma unroll
-				for (int d = -2; d <= 2; ++d)
-					any |= bit_window(fr, fd.words, fd.h, y + d, x >> 5);
-				keep = !((any >> (x & 31)) & 0x1full);
-			}
-			if (!keep) { // warp-uniform
-				const int r = replace_one(fd, x, y, &ch);
-				if (lane == 0) {
-					if (radius)
-						radius[e] = (uint8_t)(r < 255 ? r : 255);
-					if (ch && fd.rowchg) {
-						atomicOr(plane_ptr(fd, P_CHG) + (long long)y * fd.words + (x >> 5),
-							1u << (x & 31));
-						fd.rowchg[y] = 1u;
-					}
-				}
+		if (!sel && !state[t.x].replace)
+			continue; // warp-uniform
+		const FrameDesc &fd = frames[t.x];
+		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+		bool ch = false;
+		const int r = replace_one(fd, x, y, &ch);
+		if (lane == 0) {
+			if (radius)
+				radius[e] = (uint8_t)(r < 255 ? r : 255);
+			if (ch && fd.rowchg) {
+				atomicOr(plane_ptr(fd, P_CHG) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
+				fd.rowchg[y] = 1u;
 			}
 		}
 	}
@@ -629,7 +681,8 @@ fill_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__
 }
 
 // Reference src/image.cuh:50-70, in place: clean -= bg, non-finite inputs
-// restored bit for bit, uint8 mask from the bit plane.
+// restored bit for bit, uint8 mask from the bit plane.  Without a background
+// the clean pixels are already the output and are not rewritten.
 __global__ void __launch_bounds__(256)
 restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ rows, int nrows)
 {
@@ -648,6 +701,38 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 		uint8_t *mask_out = fd.mask_out + rowpix;
 		const double bgv = fd.bg;
 		const bool has_bg = fd.has_bg;
+		if (!has_bg) { // warp-uniform
+			// clean already holds the output: only the mask and the restored
+			// non-finite inputs are written, a lane per bit word (16-byte
+			// mask stores where the row's bytes are aligned).
+			const bool vec = ((uintptr_t)mask_out & 15u) == 0;
+			for (int k = lane; k < words; k += 32) {
+				const uint32_t cbits = crm[k];
+				const int x0 = 32 * k, n = min(32, w - x0);
+				if (vec && n == 32) {
+					uint4 *dst = reinterpret_cast<uint4 *>(mask_out + x0);
+#pragma unroll
+					for (int q = 0; q < 2; ++q) {
+						uint32_t v[4];
+#pragma unroll
+						for (int b = 0; b < 4; ++b) {
+							const uint32_t nib = cbits >> (16 * q + 4 * b);
+							v[b] = (nib & 1u) | ((nib >> 1) & 1u) << 8 | ((nib >> 2) & 1u) << 16 |
+							       ((nib >> 3) & 1u) << 24;
+						}
+						dst[q] = make_uint4(v[0], v[1], v[2], v[3]);
+					}
+				} else {
+					for (int i = 0; i < n; ++i)
+						mask_out[x0 + i] = (cbits >> i) & 1u;
+				}
+				for (uint32_t hb = hole[k]; hb; hb &= hb - 1) {
+					const int x = x0 + __ffs(hb) - 1;
+					clean[x] = data[x];
+				}
+			}
+			continue;
+		}
 		for (int xb = 0; xb < w; xb += 32 * ROW_UNROLL) {
 			double v[ROW_UNROLL], bg[ROW_UNROLL];
 			uint32_t hb[ROW_UNROLL], cb[ROW_UNROLL];
