@@ -150,9 +150,15 @@ CB_HD bool test_bit(const uint32_t *plane, int words, int x, int y)
 #ifdef __CUDACC__
 // Sets or clears bit `bit` of *word, for a caller that is the only writer of
 // that bit (other bits of the word may change concurrently): an atomic only
-// when the bit changes.
-__device__ __forceinline__ void write_bit(uint32_t *word, uint32_t bit, bool value)
+// when the bit changes.  `fresh`: the plane was zeroed for this pass, so only
+// a set needs an atomic and nothing is read.
+__device__ __forceinline__ void write_bit(uint32_t *word, uint32_t bit, bool value, bool fresh = false)
 {
+	if (fresh) {
+		if (value)
+			atomicOr(word, bit);
+		return;
+	}
 	const bool now = (*(volatile uint32_t *)word & bit) != 0;
 	if (value && !now)
 		atomicOr(word, bit);

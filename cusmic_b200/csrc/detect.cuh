@@ -429,11 +429,12 @@ __device__ __forceinline__ double warp_sort32(double v)
 // memory (every position it touches is in the frame, so no border mapping is
 // needed); the others read border-mapped values from global memory.
 // The warp's evaluation of the candidate at (x, y): sig over its 5 x 5
-// window, the S2 bit (and S1 unless LOW); returns sig (every lane) and the
+// window, the S2 bit (and S1 unless LOW) unless `skip`; `fresh`: the bit
+// planes were zeroed for this pass; returns sig (every lane) and the
 // noise at the pixel (nz_center).  P is the warp's 9 x 9 patch buffer.
 template <bool LOW>
 __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int y, double *P,
-	const DetectParams &prm, double &nz_center_out)
+	const DetectParams &prm, double &nz_center_out, bool fresh, bool skip = false)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
@@ -484,33 +485,36 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 		med = __shfl_sync(0xffffffffu, warp_sort32(v), 12);
 	}
 	const double sig = center - med;
-	if (lane == 0) {
+	if (lane == 0 && !skip) {
 		// Set or clear: an incremental pass keeps the bits of the previous
 		// pass and re-evaluates some pixels.
 		const long long word = (long long)y * fd.words + (x >> 5);
 		const uint32_t bit = 1u << (x & 31);
-		write_bit(plane_ptr(fd, P_S2) + word, bit, sig > prm.nb);
+		write_bit(plane_ptr(fd, P_S2) + word, bit, sig > prm.nb, fresh);
 		if (!LOW)
-			write_bit(plane_ptr(fd, P_S1) + word, bit, sig > prm.cr);
+			write_bit(plane_ptr(fd, P_S1) + word, bit, sig > prm.cr, fresh);
 	}
 	nz_center_out = nz_center;
 	return sig;
 }
 
-// candidate_sig plus the seed slot of candidate e (list-based kernels).
+// candidate_sig plus the seed slot of candidate e (list-based kernels).  A
+// hole (src/filters.cuh:137-146: sig = 0) gets no bit and no seed; its flag
+// is loaded before the evaluation and only read after it.
 template <bool LOW>
 __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, long long e, int x, int y,
-	double *P, const DetectParams &prm, Seed *seeds)
+	double *P, const DetectParams &prm, Seed *seeds, bool fresh, bool hole = false)
 {
 	double nz;
-	const double sig = candidate_sig<LOW>(fd, x, y, P, prm, nz);
+	const long long word = (long long)y * fd.words + (x >> 5);
+	const uint32_t bit = 1u << (x & 31);
+	const uint32_t excl = LOW ? 0u : plane_ptr(fd, P_EXCL)[word];
+	const double sig = candidate_sig<LOW>(fd, x, y, P, prm, nz, fresh, hole);
 	if (!LOW && (threadIdx.x & 31) == 0) {
-		const long long word = (long long)y * fd.words + (x >> 5);
-		const uint32_t bit = 1u << (x & 31);
-		const bool seed = sig > prm.cr && !(plane_ptr(fd, P_EXCL)[word] & bit);
+		const bool seed = !hole && sig > prm.cr && !(excl & bit);
 		seeds[e] = seed ? Seed{t.x, t.y, sig, nz} : Seed{NO_SEED, 0, 0.0, 0.0};
 		if (!seed) // the seed kernel decides the CAND bit of a seed
-			write_bit(plane_ptr(fd, P_CAND) + word, bit, false);
+			write_bit(plane_ptr(fd, P_CAND) + word, bit, false, fresh);
 	}
 }
 
@@ -519,24 +523,22 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 // the hole plane itself.
 __global__ void __launch_bounds__(256)
 candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
-	DetectParams prm, Control *ctl, Seed *seeds)
+	DetectParams prm, Control *ctl, Seed *seeds, int fresh)
 {
 	__shared__ double patches[8][81];
-	const int lane = threadIdx.x & 31;
 	double *P = patches[threadIdx.x >> 5];
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)ctl->n_cand;
+	uint2 next = gw < n ? cands[gw] : make_uint2(0u, 0u);
 	for (long long e = gw; e < n; e += nw) {
-		const uint2 t = cands[e];
+		const uint2 t = next;
+		if (e + nw < n) // the next entry loads during this evaluation
+			next = cands[e + nw];
 		const FrameDesc &fd = frames[t.x];
 		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
-		if (test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y)) {
-			if (lane == 0)
-				seeds[e] = Seed{NO_SEED, 0, 0.0, 0.0};
-			continue; // warp-uniform
-		}
-		candidate_eval<false>(fd, t, e, x, y, P, prm, seeds);
+		const bool hole = test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
+		candidate_eval<false>(fd, t, e, x, y, P, prm, seeds, fresh != 0, hole);
 	}
 }
 
@@ -546,7 +548,7 @@ candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 // CAND pixel) and its hole bit; the warp then evaluates the survivors.
 __global__ void __launch_bounds__(256)
 candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
-	DetectParams prm, Control *ctl)
+	DetectParams prm, Control *ctl, int fresh)
 {
 	__shared__ double patches[8][81];
 	const int lane = threadIdx.x & 31;
@@ -575,7 +577,7 @@ candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restri
 			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
 			const FrameDesc &fd = frames[tj.x];
 			candidate_eval<true>(fd, tj, base + j, (int)(tj.y % (unsigned)fd.w),
-				(int)(tj.y / (unsigned)fd.w), P, prm, nullptr);
+				(int)(tj.y / (unsigned)fd.w), P, prm, nullptr, fresh != 0);
 		}
 	}
 }
@@ -614,7 +616,7 @@ __device__ __forceinline__ double warp_rank64(double a, double b, int rank)
 // the 63 vertical triples of the patch once (T) and takes each 3 x 3 median
 // from three sorted triples (median9's rule).
 __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, double sig, double noise,
-	const DetectParams &prm, double *P, double (*T)[63])
+	const DetectParams &prm, double *P, double (*T)[63], bool fresh)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, mode = prm.mode;
@@ -673,7 +675,8 @@ __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, dou
 	fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
 	const bool cand = sig / fine > prm.contrast;
 	if (lane == 0)
-		write_bit(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31), cand);
+		write_bit(plane_ptr(fd, P_CAND) + (long long)y * fd.words + (x >> 5), 1u << (x & 31), cand,
+			fresh);
 	// Growth can flag pixels within two rows of a CAND pixel.
 	if (cand && fd.rowcand && lane < 5 && y + lane - 2 >= 0 && y + lane - 2 < h)
 		fd.rowcand[y + lane - 2] = 1u;
@@ -682,7 +685,7 @@ __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, dou
 // C (list-based): one warp per seed slot.
 __global__ void __launch_bounds__(256)
 seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds, DetectParams prm,
-	const Control *ctl)
+	const Control *ctl, int fresh)
 {
 	__shared__ double patches[8][81];
 	__shared__ double triples[8][3][63];
@@ -690,13 +693,16 @@ seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)ctl->n_cand;
+	Seed next = gw < n ? seeds[gw] : Seed{NO_SEED, 0, 0.0, 0.0};
 	for (long long e = gw; e < n; e += nw) {
-		const Seed sd = seeds[e];
+		const Seed sd = next;
+		if (e + nw < n) // the next slot loads during this evaluation
+			next = seeds[e + nw];
 		if (sd.frame == NO_SEED)
 			continue; // warp-uniform
 		const FrameDesc &fd = frames[sd.frame];
 		seed_eval(fd, (int)(sd.pixel % (unsigned)fd.w), (int)(sd.pixel / (unsigned)fd.w), sd.sig,
-			sd.noise, prm, patches[warp], triples[warp]);
+			sd.noise, prm, patches[warp], triples[warp], fresh != 0);
 	}
 }
 

@@ -541,11 +541,12 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 		mark(rec, K_CLASSIFY);
 	}
 	candidate_high_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
-		ws.seeds.p);
+		ws.seeds.p, !incremental);
 	mark(rec, K_CAND);
-	seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p);
+	seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p, !incremental);
 	mark(rec, K_SEED);
-	candidate_low_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p);
+	candidate_low_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
+		!incremental);
 	mark(rec, K_LOW);
 	// An incremental pass grows on its dirty rows only.
 	grow_update_kernel<<<grid_for_rows(di, nrows, rowb), 256, 0, s>>>(ws.frames.p, ws.state.p,
@@ -1300,9 +1301,10 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 					sig_model_kernel<<<b, 256, 0, s>>>(frames, state, items, L.nitems, prm, ctl,
 						cands);
 				}
-				candidate_high_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds);
-				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl);
-				candidate_low_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl);
+				// The dense kernels above zeroed S1, S2 and CAND.
+				candidate_high_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds, 1);
+				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl, 1);
+				candidate_low_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, 1);
 				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, nullptr, targets,
 					ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
