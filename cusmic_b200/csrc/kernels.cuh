@@ -517,10 +517,13 @@ __device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y, bo
 			bool d = false;
 			double v = INFINITY;
 			if (lane < area) {
+				// The value loads with the donor bits and is dropped for a
+				// non-donor (whose pixel another warp may be writing).
 				int cx = win.x0 + lane % ww, cy = win.y0 + lane / ww;
+				const double c = fd.clean[(long long)cy * w + cx];
 				d = donor_at(don, crm, words, cx, cy);
 				if (d)
-					v = fd.clean[(long long)cy * w + cx];
+					v = c;
 			}
 			nd = __popc(__ballot_sync(0xffffffffu, d));
 			if (!nd)
