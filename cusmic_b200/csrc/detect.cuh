@@ -432,14 +432,32 @@ __device__ __forceinline__ double warp_sort32(double v)
 // window, the S2 bit (and S1 unless LOW) unless `skip`; `fresh`: the bit
 // planes were zeroed for this pass; returns sig (every lane) and the
 // noise at the pixel (nz_center).  P is the warp's 9 x 9 patch buffer.
-template <bool LOW>
+// Which frames a kernel variant serves: any (decided per frame), error-map
+// frames only, or noise-model frames only (a variant compiles one path and
+// needs fewer registers).
+enum FramePath { PATH_ANY = 0, PATH_ERROR = 1, PATH_MODEL = 2 };
+
+template <int PATH>
+__device__ __forceinline__ bool has_error_map(const FrameDesc &fd)
+{
+	return PATH == PATH_ERROR ? true : PATH == PATH_MODEL ? false : fd.error != nullptr;
+}
+
+template <int PATH>
+__device__ __forceinline__ bool serves(const FrameDesc &fd)
+{
+	return PATH == PATH_ANY || (fd.error != nullptr) == (PATH == PATH_ERROR);
+}
+
+template <bool LOW, int PATH = PATH_ANY>
 __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int y, double *P,
 	const DetectParams &prm, double &nz_center_out, bool fresh, bool skip = false)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
+	const bool err = has_error_map<PATH>(fd);
 	double v = INFINITY, nz = 0;
-	if (!fd.error && x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+	if (!err && x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
 		__syncwarp();
 		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
 		for (int k = lane; k < 81; k += 32)
@@ -464,7 +482,7 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 		v = 0;
 		if (mx >= 0 && my >= 0) {
 			const long long i = (long long)my * w + mx;
-			nz = fd.error ? fd.error[i] : noise_model_at(fd, mx, my, mode);
+			nz = err ? fd.error[i] : noise_model_at(fd, mx, my, mode);
 			const double lap = lap_formula(fd.clean[i], clean_at(fd, mx, my - 1, lm),
 				clean_at(fd, mx, my + 1, lm), clean_at(fd, mx - 1, my, lm),
 				clean_at(fd, mx + 1, my, lm));
@@ -501,7 +519,7 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 // candidate_sig plus the seed slot of candidate e (list-based kernels).  A
 // hole (src/filters.cuh:137-146: sig = 0) gets no bit and no seed; its flag
 // is loaded before the evaluation and only read after it.
-template <bool LOW>
+template <bool LOW, int PATH = PATH_ANY>
 __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, long long e, int x, int y,
 	double *P, const DetectParams &prm, Seed *seeds, bool fresh, bool hole = false)
 {
@@ -509,7 +527,7 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 	const long long word = (long long)y * fd.words + (x >> 5);
 	const uint32_t bit = 1u << (x & 31);
 	const uint32_t excl = LOW ? 0u : plane_ptr(fd, P_EXCL)[word];
-	const double sig = candidate_sig<LOW>(fd, x, y, P, prm, nz, fresh, hole);
+	const double sig = candidate_sig<LOW, PATH>(fd, x, y, P, prm, nz, fresh, hole);
 	if (!LOW && (threadIdx.x & 31) == 0) {
 		const bool seed = !hole && sig > prm.cr && !(excl & bit);
 		seeds[e] = seed ? Seed{t.x, t.y, sig, nz} : Seed{NO_SEED, 0, 0.0, 0.0};
@@ -521,7 +539,10 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 // B, high list: one warp per candidate.  Holes have sig = 0
 // (src/filters.cuh:137-146): no bit, no seed; the dense kernel does not test
 // the hole plane itself.
-__global__ void __launch_bounds__(256)
+// PATH: the frames this launch serves (FramePath); the other launch of a
+// mixed batch takes the rest of the list.
+template <int PATH>
+__global__ void __launch_bounds__(256, PATH == PATH_ERROR ? 4 : 3)
 candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, Seed *seeds, int fresh)
 {
@@ -536,9 +557,11 @@ candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 		if (e + nw < n) // the next entry loads during this evaluation
 			next = cands[e + nw];
 		const FrameDesc &fd = frames[t.x];
+		if (!serves<PATH>(fd))
+			continue; // warp-uniform
 		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
 		const bool hole = test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
-		candidate_eval<false>(fd, t, e, x, y, P, prm, seeds, fresh != 0, hole);
+		candidate_eval<false, PATH>(fd, t, e, x, y, P, prm, seeds, fresh != 0, hole);
 	}
 }
 
@@ -546,7 +569,8 @@ candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 // its clipped 5 x 5 neighbourhood of the CAND plane with five 36-bit row
 // windows (S2 is read only by the second growth step, within distance 2 of a
 // CAND pixel) and its hole bit; the warp then evaluates the survivors.
-__global__ void __launch_bounds__(256)
+template <int PATH>
+__global__ void __launch_bounds__(256, PATH == PATH_ERROR ? 4 : 3)
 candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, int fresh)
 {
@@ -570,13 +594,14 @@ candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restri
 #pragma unroll
 			for (int d = -2; d <= 2; ++d)
 				any |= bit_window(cand, fd.words, fd.h, y + d, x >> 5);
-			near = ((any >> (x & 31)) & 0x1full) && !test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
+			near = serves<PATH>(fd) && ((any >> (x & 31)) & 0x1full) &&
+				!test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
 		}
 		for (unsigned m = __ballot_sync(0xffffffffu, near); m; m &= m - 1) {
 			const int j = __ffs(m) - 1;
 			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
 			const FrameDesc &fd = frames[tj.x];
-			candidate_eval<true>(fd, tj, base + j, (int)(tj.y % (unsigned)fd.w),
+			candidate_eval<true, PATH>(fd, tj, base + j, (int)(tj.y % (unsigned)fd.w),
 				(int)(tj.y / (unsigned)fd.w), P, prm, nullptr, fresh != 0);
 		}
 	}

@@ -540,13 +540,23 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 			ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
 		mark(rec, K_CLASSIFY);
 	}
-	candidate_high_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
-		ws.seeds.p, !incremental);
+	// One launch per kind of frame in the batch: each variant compiles only
+	// its noise path (error map or noise model).
+	if (L.error_frames)
+		candidate_high_kernel<PATH_ERROR><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
+			ws.ctl.p, ws.seeds.p, !incremental);
+	if (L.error_frames < nf)
+		candidate_high_kernel<PATH_MODEL><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
+			ws.ctl.p, ws.seeds.p, !incremental);
 	mark(rec, K_CAND);
 	seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p, !incremental);
 	mark(rec, K_SEED);
-	candidate_low_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p,
-		!incremental);
+	if (L.error_frames)
+		candidate_low_kernel<PATH_ERROR><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
+			ws.ctl.p, !incremental);
+	if (L.error_frames < nf)
+		candidate_low_kernel<PATH_MODEL><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
+			ws.ctl.p, !incremental);
 	mark(rec, K_LOW);
 	// An incremental pass grows on its dirty rows only.
 	grow_update_kernel<<<grid_for_rows(di, nrows, rowb), 256, 0, s>>>(ws.frames.p, ws.state.p,
@@ -1302,9 +1312,10 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 						cands);
 				}
 				// The dense kernels above zeroed S1, S2 and CAND.
-				candidate_high_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, seeds, 1);
+				candidate_high_kernel<PATH_ANY><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl,
+					seeds, 1);
 				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl, 1);
-				candidate_low_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, 1);
+				candidate_low_kernel<PATH_ANY><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, 1);
 				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, nullptr, targets,
 					ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
