@@ -731,4 +731,48 @@ seed_kernel(const FrameDesc *__restrict__ frames, const Seed *__restrict__ seeds
 	}
 }
 
+// B and C fused, high list: one warp per candidate, and a candidate that is
+// a seed gets its fine-structure test from the same warp at once (it needs
+// only its own sig and noise and the clean pixels within 4), so no seed list
+// is walked.  PATH as for candidate_high_kernel (error-map frames use it;
+// noise-model candidates cost more and balance better as two kernels).  With
+// `seeds` (a batch that also runs seed_kernel) each served entry's slot is
+// marked empty.
+template <int PATH>
+__global__ void __launch_bounds__(256, PATH == PATH_ERROR ? 4 : 3)
+candidate_seed_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
+	DetectParams prm, Control *ctl, Seed *seeds, int fresh)
+{
+	__shared__ double patches[8][81];
+	__shared__ double triples[8][3][63];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	double *P = patches[warp];
+	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	const long long n = (long long)ctl->n_cand;
+	uint2 next = gw < n ? cands[gw] : make_uint2(0u, 0u);
+	for (long long e = gw; e < n; e += nw) {
+		const uint2 t = next;
+		if (e + nw < n) // the next entry loads during this evaluation
+			next = cands[e + nw];
+		const FrameDesc &fd = frames[t.x];
+		if (!serves<PATH>(fd))
+			continue; // warp-uniform
+		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+		const long long word = (long long)y * fd.words + (x >> 5);
+		const uint32_t bit = 1u << (x & 31);
+		const bool hole = (plane_ptr(fd, P_HOLE)[word] & bit) != 0;
+		const uint32_t excl = plane_ptr(fd, P_EXCL)[word];
+		if (seeds && lane == 0)
+			seeds[e] = Seed{NO_SEED, 0, 0.0, 0.0};
+		double nz;
+		const double sig = candidate_sig<false, PATH>(fd, x, y, P, prm, nz, fresh != 0, hole);
+		// Every lane holds the same sig, so the branch is warp-uniform.
+		if (!hole && sig > prm.cr && !(excl & bit))
+			seed_eval(fd, x, y, sig, nz, prm, P, triples[warp], fresh != 0);
+		else if (lane == 0)
+			write_bit(plane_ptr(fd, P_CAND) + word, bit, false, fresh != 0);
+	}
+}
+
 } // namespace cb

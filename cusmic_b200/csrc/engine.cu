@@ -165,8 +165,8 @@ struct Workspace {
 	DevBuf<uint8_t> radius; // per target: window radius of its last replacement
 	DevBuf<int2> dirty;     // dirty-row list of an incremental pass
 	DevBuf<unsigned> sel;   // targets the replacement after a pass visits
+	DevBuf<Seed> seeds;     // seed slots of the noise-model candidates
 	DevBuf<uint2> cands;
-	DevBuf<Seed> seeds;
 	DevBuf<int4> bulk;
 	DevBuf<FloorJob> jobs;
 	DevBuf<BlockFloor> floors;
@@ -414,8 +414,9 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 		ws.radius.ensure(L.total_px);
 		ws.dirty.ensure(L.rows.size());
 		ws.sel.ensure(L.total_px);
+		if (L.error_frames < (int)nf)
+			ws.seeds.ensure(L.total_px);
 		ws.cands.ensure(L.total_px);
-		ws.seeds.ensure(L.total_px);
 		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
 		ws.pre_counts.ensure(L.bulk.size() * BK_CWARPS);
 	}
@@ -541,16 +542,20 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 		mark(rec, K_CLASSIFY);
 	}
 	// One launch per kind of frame in the batch: each variant compiles only
-	// its noise path (error map or noise model).
+	// its noise path (error map or noise model).  Error-map seeds are tested
+	// by the candidate's own warp; noise-model seeds by seed_kernel.
+	const bool model = L.error_frames < nf;
 	if (L.error_frames)
-		candidate_high_kernel<PATH_ERROR><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
-			ws.ctl.p, ws.seeds.p, !incremental);
-	if (L.error_frames < nf)
+		candidate_seed_kernel<PATH_ERROR><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
+			ws.ctl.p, model ? ws.seeds.p : nullptr, !incremental);
+	if (model)
 		candidate_high_kernel<PATH_MODEL><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
 			ws.ctl.p, ws.seeds.p, !incremental);
 	mark(rec, K_CAND);
-	seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p, !incremental);
-	mark(rec, K_SEED);
+	if (model) {
+		seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p, !incremental);
+		mark(rec, K_SEED);
+	}
 	if (L.error_frames)
 		candidate_low_kernel<PATH_ERROR><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
 			ws.ctl.p, !incremental);
