@@ -440,3 +440,23 @@ def test_incremental_passes_ragged_stops(cuda, oracle):
         frames.append(dict(data=data, error=np.sqrt(np.abs(data) / 1.5 + 16)))
     check_against_oracle(oracle, frames, dict(contrast=1.0, cr_threshold=4.0,
                                               neighbor_threshold=1.5, maxiter=6), ragged=True)
+
+
+@pytest.mark.parametrize("mode", ("mirror", "wrap", "constant"))
+def test_ragged_mixed_error_maps_and_noise_model(cuda, oracle, mode):
+    """Error-map and noise-model frames in one ragged batch: each kind runs its
+    own candidate kernel, noise-model seeds go through the seed list and the
+    error-map entries of that list stay empty."""
+    frames = []
+    for i, (h, w) in enumerate(((40, 300), (33, 130), (64, 96), (17, 33), (50, 514), (9, 7))):
+        if i % 3 == 0:
+            data = clustered_scene(700 + i, h, w)
+        else:
+            data = small_scene(700 + i, h, w, holes=0.005, rays=max(2, h * w // 60))[0]
+        f = dict(data=data)
+        if i % 2 == 0:
+            f["error"] = np.sqrt(np.abs(np.nan_to_num(data)) / 1.5 + 16)
+        else:
+            f.update(gain=1.0 + 0.5 * i, readnoise=3.0 + i)
+        frames.append(f)
+    check_against_oracle(oracle, frames, dict(SETTINGS, border=mode, maxiter=5), ragged=True)
