@@ -122,7 +122,7 @@ struct FrameState {
 // Loop control shared by the per-pass kernels.
 struct Control {
 	unsigned long long n_targets; // length of the target list
-	unsigned long long n_holes;   // length of the hole list (front of the same buffer)
+	unsigned long long n_holes;   // length of the hole list prepare_kernel writes
 	unsigned long long n_cand;    // this pass: pixels whose sig_raw can exceed cr_threshold
 	unsigned long long n_low;     // this pass: pixels whose sig_raw can only exceed neighbor
 	unsigned long long cand_cap;  // capacity of the candidate buffer (high from the front,

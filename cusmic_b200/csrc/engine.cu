@@ -594,9 +594,11 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	check(cudaMemsetAsync(ws.bits.p, 0, (size_t)L.total_words * sizeof(uint32_t), s));
 	check(cudaMemsetAsync(ws.rowmarks.p, 0, 2 * (size_t)L.row_words * sizeof(uint32_t), s));
 	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
-		nrows);
+		nrows, ws.ctl.p, ws.cands.p);
 	mark(rec, K_PREPARE);
-	fill_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows);
+	// The hole list lives in the candidate buffer until the first pass.
+	fill_list_kernel<<<di.sms * L.tune.sparse_blocks_per_sm, 256, 0, s>>>(ws.frames.p, ws.state.p,
+		ws.cands.p, &ws.ctl.p->n_holes);
 	mark(rec, K_FILL);
 	// Block floors (error-map thresholds; noise-model keys of the filled
 	// frames, which replacement keeps as lower bounds).

@@ -141,7 +141,8 @@ constexpr int ROW_UNROLL = 4;
 // stores below go through pointers the compiler cannot prove distinct from
 // them).
 template <bool MASK, bool BGMAP>
-__device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st, int y)
+__device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st, int f, int y,
+	Control *ctl, uint2 *holes)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, words = fd.words;
@@ -215,6 +216,11 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 			excl_plane[k] = my_e;
 			donor_plane[k] = my_d;
 		}
+		if (holes && __any_sync(0xffffffffu, my_h != 0)) { // list the segment's holes for the fill
+			unsigned long long slot = warp_append(&ctl->n_holes, __popc(my_h));
+			for (uint32_t b = my_h; b; b &= b - 1)
+				holes[slot++] = make_uint2((unsigned)f, (unsigned)(rowpix + 32 * k + __ffs(b) - 1));
+		}
 	}
 	if (lane == 0) {
 		if (any_hole)
@@ -235,7 +241,7 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 // fill scans the HOLE plane.
 __global__ void __launch_bounds__(256, 4)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
-	int nrows)
+	int nrows, Control *ctl = nullptr, uint2 *holes = nullptr)
 {
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
 	for (int r = gw; r < nrows; r += nw) {
@@ -244,11 +250,11 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 		FrameState &st = state[item.x];
 		const bool mask = fd.mask, bgmap = fd.bg_map;
 		if (mask && !bgmap)
-			prepare_row<true, false>(fd, st, item.y);
+			prepare_row<true, false>(fd, st, item.x, item.y, ctl, holes);
 		else if (!mask && !bgmap)
-			prepare_row<false, false>(fd, st, item.y);
+			prepare_row<false, false>(fd, st, item.x, item.y, ctl, holes);
 		else
-			prepare_row<true, true>(fd, st, item.y);
+			prepare_row<true, true>(fd, st, item.x, item.y, ctl, holes);
 	}
 }
 
@@ -658,7 +664,26 @@ replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restric
 }
 
 // Initial fill of non-finite pixels (src/cleaner.cuh:78-100) for frames with
-// a finite donor: one warp per row scans the row's HOLE words.
+// a finite donor, from the hole list prepare_kernel wrote: one warp per hole
+// (holes are never donors, so the order does not matter).
+__global__ void __launch_bounds__(256)
+fill_list_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
+	const uint2 *__restrict__ holes, const unsigned long long *count)
+{
+	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	const long long n = (long long)*count;
+	for (long long e = gw; e < n; e += nw) {
+		const uint2 t = holes[e];
+		if (!state[t.x].finite)
+			continue; // warp-uniform
+		const FrameDesc &fd = frames[t.x];
+		replace_one(fd, (int)(t.y % (unsigned)fd.w), (int)(t.y / (unsigned)fd.w));
+	}
+}
+
+// The same fill without a hole list: one warp per row scans the row's HOLE
+// words.
 __global__ void __launch_bounds__(256)
 fill_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const int2 *__restrict__ rows, int nrows)
