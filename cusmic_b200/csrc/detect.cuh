@@ -542,7 +542,7 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 // PATH: the frames this launch serves (FramePath); the other launch of a
 // mixed batch takes the rest of the list.
 template <int PATH>
-__global__ void __launch_bounds__(256, PATH == PATH_ERROR ? 4 : 3)
+__global__ void __launch_bounds__(256, 4)
 candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, Seed *seeds, int fresh)
 {
