@@ -9,9 +9,11 @@
 //    32 x 32 block, turned into a threshold T = 2 min(cr, nb) (1 - 1e-12) x
 //    floor.  With an error map floor_kernel takes min(max(error, 0)) over the
 //    block (NaN counts as 0), once for each distinct map.  With the noise
-//    model (src/filters.cuh:107-123) it stores, after the hole fill, the
-//    smallest clean value of the block (as an ordered key) and the block's
-//    largest gain and smallest read noise when they are maps.  Between passes
+//    model (src/filters.cuh:107-123) it stores a lower bound of the block's
+//    clean values as an ordered key (from the row minima prepare_kernel keeps
+//    of the non-hole pixels; the hole fill lowers it with the values it
+//    writes) and the block's largest gain and smallest read noise when they
+//    are maps.  Between passes
 //    only replacement changes clean,
 //    and replace_kernel lowers the key of the block it writes into, so the key
 //    stays a lower bound of the block's values.  Every 5 x 5 median window of
@@ -249,9 +251,17 @@ CB_HD BulkRow bulk_row(int w, int h, int lm, int mis, int x0, int r)
 }
 
 // Floors of 32 x 32 blocks (see the head of this file): of each distinct
-// error map, and (after the hole fill, when every clean value is finite) of
-// each noise-model frame.  One warp per block, one lane per column, all 32
-// rows in flight.
+// error map (one lane per column, all 32 rows in flight), and of each
+// noise-model frame (from prepare_kernel's row minima, one lane per row).
+// One warp per block.
+//
+// Noise-model blocks of frames without gain or read-noise maps are left to
+// model_floor_kernel.
+__device__ __forceinline__ bool thread_floor_job(const FloorJob &jb, const FrameDesc &fd)
+{
+	return jb.kind && !fd.gain_map && !fd.rn_map;
+}
+
 __global__ void __launch_bounds__(256)
 floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
 	DetectParams prm, BlockFloor *floors)
@@ -262,19 +272,23 @@ floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ 
 	for (int j = gw; j < njobs; j += nw) {
 		const FloorJob jb = jobs[j];
 		const FrameDesc &fd = frames[jb.frame];
+		if (thread_floor_job(jb, fd))
+			continue; // warp-uniform
 		const int w = fd.w, x = jb.x0 + lane;
 		const int n = (jb.y0 + FLOOR_BLOCK < fd.h ? jb.y0 + FLOOR_BLOCK : fd.h) - jb.y0;
 		if (jb.kind) { // noise model: ordered keys of clean, -gain, read noise
 			const long long at = (long long)jb.y0 * w + x;
 			unsigned long long key = ~0ull, gkey = ~0ull, rkey = ~0ull;
-			double v[FLOOR_BLOCK];
-#pragma unroll
-			for (int k = 0; k < FLOOR_BLOCK; ++k)
-				v[k] = x < w && k < n ? fd.clean[at + (long long)k * w] : 0.0;
-#pragma unroll
-			for (int k = 0; k < FLOOR_BLOCK; ++k)
-				if (x < w && k < n)
-					key = min(key, order_key(v[k]));
+			// Clean: the smallest of the block rows' high words (prepare_kernel;
+			// lane = row), as a key with its low word cleared: no larger than
+			// the smallest key of the block's non-hole values.
+			{
+				const uint32_t m = lane < n ? plane_ptr(fd, P_ROWMIN)[(long long)(jb.y0 + lane) * fd.words +
+					jb.x0 / 32] : 0xffffffffu;
+				const uint32_t hi = __reduce_min_sync(0xffffffffu, m);
+				if (hi != 0xffffffffu)
+					key = (unsigned long long)hi << 32;
+			}
 			if (x < w && (fd.gain_map || fd.rn_map))
 				for (int k = 0; k < n; ++k) {
 					if (fd.gain_map)
@@ -307,6 +321,29 @@ floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ 
 		const double T = tmin2 * m;
 		if (lane == 0)
 			floors[jb.out].thr = T >= 0 ? T : 0.0; // NaN lists everything
+	}
+}
+
+// Floors of the noise-model blocks of frames without gain or read-noise maps,
+// one thread per block: the smallest of the block rows' high words
+// (prepare_kernel's row minima) as a key with its low word cleared.
+__global__ void __launch_bounds__(256)
+model_floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
+	BlockFloor *floors)
+{
+	for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) {
+		const FloorJob jb = jobs[j];
+		const FrameDesc &fd = frames[jb.frame];
+		if (!thread_floor_job(jb, fd))
+			continue;
+		const int n = min(FLOOR_BLOCK, fd.h - jb.y0);
+		const uint32_t *m = plane_ptr(fd, P_ROWMIN) + (long long)jb.y0 * fd.words + jb.x0 / 32;
+		uint32_t hi = 0xffffffffu;
+#pragma unroll 8
+		for (int k = 0; k < n; ++k)
+			hi = min(hi, m[(long long)k * fd.words]);
+		floors[jb.out] = BlockFloor{0.0, hi != 0xffffffffu ? (unsigned long long)hi << 32 : ~0ull,
+			~0ull, ~0ull};
 	}
 }
 

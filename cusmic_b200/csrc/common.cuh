@@ -41,6 +41,8 @@ enum Plane {
 	P_CAND,   // seed: S1, not excluded, contrast test passed
 	P_FRESH,  // pixels the last growth step added to the mask
 	P_CHG,    // pixels whose value the last replacement changed
+	P_ROWMIN, // noise-model frames: per row and bit word, the smallest high word of
+	          // the ordered keys of its finite input pixels (all ones: none)
 	N_PLANES
 };
 

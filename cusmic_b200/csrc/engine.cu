@@ -596,18 +596,22 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
 		nrows, ws.ctl.p, ws.cands.p);
 	mark(rec, K_PREPARE);
-	// The hole list lives in the candidate buffer until the first pass.
-	fill_list_kernel<<<di.sms * L.tune.sparse_blocks_per_sm, 256, 0, s>>>(ws.frames.p, ws.state.p,
-		ws.cands.p, &ws.ctl.p->n_holes);
-	mark(rec, K_FILL);
-	// Block floors (error-map thresholds; noise-model keys of the filled
-	// frames, which replacement keeps as lower bounds).
+	// Block floors: error-map thresholds; noise-model keys from prepare's row
+	// minima of the non-hole pixels, which the hole fill and every later
+	// replacement lower with the values they write.
 	if (!L.jobs.empty()) {
 		const int nj = (int)L.jobs.size(), cap = di.sms * 8;
 		floor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p, ws.jobs.p,
 			nj, L.prm, ws.floors.p);
+		if (L.error_frames < nf)
+			model_floor_kernel<<<(nj + 255) / 256 < cap ? (nj + 255) / 256 : cap, 256, 0, s>>>(
+				ws.frames.p, ws.jobs.p, nj, ws.floors.p);
 		mark(rec, K_FLOOR);
 	}
+	// The hole list lives in the candidate buffer until the first pass.
+	fill_list_kernel<<<di.sms * L.tune.sparse_blocks_per_sm, 256, 0, s>>>(ws.frames.p, ws.state.p,
+		ws.cands.p, &ws.ctl.p->n_holes);
+	mark(rec, K_FILL);
 }
 
 static void launch_epilogue(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,

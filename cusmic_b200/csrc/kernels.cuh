@@ -140,7 +140,7 @@ constexpr int ROW_UNROLL = 4;
 // mask, BGMAP = background map.  Descriptor fields are held in registers (the
 // stores below go through pointers the compiler cannot prove distinct from
 // them).
-template <bool MASK, bool BGMAP>
+template <bool MASK, bool BGMAP, bool ROWMIN>
 __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st, int f, int y,
 	Control *ctl, uint2 *holes)
 {
@@ -158,8 +158,12 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 	uint32_t *donor_plane = plane_ptr(fd, P_DONOR) + roww;
 	uint32_t any_hole = 0, any_allowed = 0, any_finite = 0;
 	int ndonor = 0;
+	// Noise-model frames with floors: per bit word the smallest high word of
+	// the ordered keys of the non-hole clean values (a lower bound for the
+	// block floors, which the hole fill then lowers with the values it writes).
+	uint32_t *rowmin = ROWMIN ? plane_ptr(fd, P_ROWMIN) + roww : nullptr;
 	for (int seg = 0; seg * 1024 < w; ++seg) {
-		uint32_t my_h = 0, my_e = 0, my_d = 0;
+		uint32_t my_h = 0, my_e = 0, my_d = 0, my_m = 0xffffffffu;
 		for (int c0 = 0; c0 < 32; c0 += ROW_UNROLL) {
 			const int xb = seg * 1024 + c0 * 32;
 			if (xb >= w)
@@ -197,6 +201,10 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 					donor = ok && isfinite(c);
 				}
 				const uint32_t hw = __ballot_sync(0xffffffffu, hole);
+				uint32_t mw = 0xffffffffu;
+				if (ROWMIN)
+					mw = __reduce_min_sync(0xffffffffu,
+						valid && !hole ? (uint32_t)(order_key(c) >> 32) : 0xffffffffu);
 				const uint32_t ew = __ballot_sync(0xffffffffu, valid && !ok);
 				const uint32_t dw = __ballot_sync(0xffffffffu, donor);
 				any_allowed |= __ballot_sync(0xffffffffu, ok);
@@ -207,6 +215,7 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 					my_h = hw;
 					my_e = ew;
 					my_d = dw;
+					my_m = mw;
 				}
 			}
 		}
@@ -215,6 +224,8 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 			hole_plane[k] = my_h;
 			excl_plane[k] = my_e;
 			donor_plane[k] = my_d;
+			if (ROWMIN)
+				rowmin[k] = my_m;
 		}
 		if (holes && __any_sync(0xffffffffu, my_h != 0)) { // list the segment's holes for the fill
 			unsigned long long slot = warp_append(&ctl->n_holes, __popc(my_h));
@@ -249,12 +260,18 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 		const FrameDesc &fd = frames[item.x];
 		FrameState &st = state[item.x];
 		const bool mask = fd.mask, bgmap = fd.bg_map;
-		if (mask && !bgmap)
-			prepare_row<true, false>(fd, st, item.x, item.y, ctl, holes);
-		else if (!mask && !bgmap)
-			prepare_row<false, false>(fd, st, item.x, item.y, ctl, holes);
-		else
-			prepare_row<true, true>(fd, st, item.x, item.y, ctl, holes);
+		if (fd.floors && !fd.error) { // noise-model frame: row minima for the floors
+			if (!mask && !bgmap)
+				prepare_row<false, false, true>(fd, st, item.x, item.y, ctl, holes);
+			else
+				prepare_row<true, true, true>(fd, st, item.x, item.y, ctl, holes);
+		} else if (mask && !bgmap) {
+			prepare_row<true, false, false>(fd, st, item.x, item.y, ctl, holes);
+		} else if (!mask && !bgmap) {
+			prepare_row<false, false, false>(fd, st, item.x, item.y, ctl, holes);
+		} else {
+			prepare_row<true, true, false>(fd, st, item.x, item.y, ctl, holes);
+		}
 	}
 }
 
