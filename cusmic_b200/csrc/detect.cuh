@@ -424,10 +424,12 @@ __device__ __forceinline__ double warp_sort32(double v)
 // the second growth step, i.e. within distance 2 of a CAND pixel; candidates
 // with no CAND bit in their clipped 5 x 5 neighbourhood are skipped.
 //
-// On noise-model frames a candidate at least 4 pixels from every edge reads
-// its 25 noise windows from a 9 x 9 patch of clean staged in the warp's shared
-// memory (every position it touches is in the frame, so no border mapping is
-// needed); the others read border-mapped values from global memory.
+// A candidate at least 4 pixels from every edge stages the 9 x 9 patch of
+// clean around it in the warp's shared memory (every position it touches is
+// in the frame, so no border mapping is needed) and takes its Laplacians and,
+// on noise-model frames, its 25 noise windows from it; the others read
+// border-mapped values from global memory.  The patch stays for a seed test
+// of the same pixel.
 // The warp's evaluation of the candidate at (x, y): sig over its 5 x 5
 // window, the S2 bit (and S1 unless LOW) unless `skip`; `fresh`: the bit
 // planes were zeroed for this pass; returns sig (every lane) and the
@@ -457,23 +459,27 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
 	const bool err = has_error_map<PATH>(fd);
 	double v = INFINITY, nz = 0;
-	if (!err && x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+	if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
 		__syncwarp();
 		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
 		for (int k = lane; k < 81; k += 32)
 			P[k] = src[(long long)(k / 9) * w + k % 9];
+		if (lane < 25 && err) // loads with the patch
+			nz = fd.error[(long long)(y + lane / 5 - 2) * w + x + lane % 5 - 2];
 		__syncwarp();
 		if (lane < 25) {
 			const int dy = lane / 5, dx = lane % 5;
 			const double *q = P + (dy + 2) * 9 + dx + 2; // the window cell
-			const long long i = (long long)(y + dy - 2) * w + x + dx - 2;
-			double win[25];
+			if (!err) {
+				const long long i = (long long)(y + dy - 2) * w + x + dx - 2;
+				double win[25];
 #pragma unroll
-			for (int a = 0; a < 5; ++a)
+				for (int a = 0; a < 5; ++a)
 #pragma unroll
-				for (int b = 0; b < 5; ++b)
-					win[a * 5 + b] = q[(a - 2) * 9 + b - 2];
-			nz = noise_from_median(fd, i, median_network(win));
+					for (int b = 0; b < 5; ++b)
+						win[a * 5 + b] = q[(a - 2) * 9 + b - 2];
+				nz = noise_from_median(fd, i, median_network(win));
+			}
 			v = lap_formula(q[0], q[-9], q[9], q[-1], q[1]) / (2 * nz);
 		}
 	} else if (lane < 25) {
@@ -641,17 +647,19 @@ __device__ __forceinline__ double warp_rank64(double a, double b, int rank)
 // the 63 vertical triples of the patch once (T) and takes each 3 x 3 median
 // from three sorted triples (median9's rule).
 __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, double sig, double noise,
-	const DetectParams &prm, double *P, double (*T)[63], bool fresh)
+	const DetectParams &prm, double *P, double (*T)[63], bool fresh, bool staged = false)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, mode = prm.mode;
 	double m3[2] = {INFINITY, INFINITY};
 	if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
 		__syncwarp();
-		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
-		for (int k = lane; k < 81; k += 32)
-			P[k] = src[(long long)(k / 9) * w + k % 9];
-		__syncwarp();
+		if (!staged) { // else the candidate evaluation left this patch in P
+			const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
+			for (int k = lane; k < 81; k += 32)
+				P[k] = src[(long long)(k / 9) * w + k % 9];
+			__syncwarp();
+		}
 		for (int k = lane; k < 63; k += 32) {
 			double a = P[k], b = P[k + 9], c = P[k + 18];
 			cas(a, b);
@@ -769,7 +777,7 @@ candidate_seed_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 		const double sig = candidate_sig<false, PATH>(fd, x, y, P, prm, nz, fresh != 0, hole);
 		// Every lane holds the same sig, so the branch is warp-uniform.
 		if (!hole && sig > prm.cr && !(excl & bit))
-			seed_eval(fd, x, y, sig, nz, prm, P, triples[warp], fresh != 0);
+			seed_eval(fd, x, y, sig, nz, prm, P, triples[warp], fresh != 0, true);
 		else if (lane == 0)
 			write_bit(plane_ptr(fd, P_CAND) + word, bit, false, fresh != 0);
 	}
