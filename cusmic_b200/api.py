@@ -68,6 +68,10 @@ class Image:
         self.data = data if data.is_cuda else data.to(device)
         shape, frame = tuple(self.data.shape), tuple(self.data.shape[-2:])
         fields = ("error",) if self.error is not None else ("effective_gain", "readnoise")
+        # The content checks of every map run on the device and are read back
+        # with one copy (one host synchronisation per Image, on the current
+        # stream); the first failing check, in the reference's order, raises.
+        checks = []
         with torch.cuda.device(device):
             for name in (*fields, "background"):
                 value = getattr(self, name)
@@ -81,13 +85,17 @@ class Image:
                 if tuple(value.shape) not in (shape, frame) and (name == "error" or value.dim() != 0):
                     raise ValueError(f"{name} has an incompatible shape")
                 value = value.to(torch.float64)
-                if not bool(torch.isfinite(value).all()):
-                    raise ValueError(f"{name} must be finite")
-                if name in ("error", "effective_gain") and bool((value <= 0).any()):
-                    raise ValueError(f"{name} must be positive")
-                if name == "readnoise" and bool((value < 0).any()):
-                    raise ValueError("readnoise must be nonnegative")
+                checks.append((~torch.isfinite(value).all(), f"{name} must be finite"))
+                if name in ("error", "effective_gain"):
+                    checks.append(((value <= 0).any(), f"{name} must be positive"))
+                if name == "readnoise":
+                    checks.append(((value < 0).any(), "readnoise must be nonnegative"))
                 setattr(self, name, value)
+            if checks:
+                failed = torch.stack([flag for flag, _ in checks]).cpu().tolist()
+                for bad, (_, message) in zip(failed, checks):
+                    if bad:
+                        raise ValueError(message)
             if self.mask is not None:
                 self.mask = _as_tensor(self.mask, device).to(torch.bool)
                 if tuple(self.mask.shape) not in (shape, frame):

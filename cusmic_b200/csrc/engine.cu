@@ -19,14 +19,17 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #ifndef CUSMIC_B200_VERSION
@@ -95,6 +98,187 @@ template <class T> struct PinBuf {
 	{
 		if (p)
 			cudaFreeHost(p);
+	}
+};
+
+// Host threads that copy between the caller's pageable buffers and pinned
+// staging memory for the host entry point: a copy is split over the workers
+// and the calling thread (one pool per process, shared by concurrent calls).
+class CopyPool {
+public:
+	static CopyPool &get()
+	{
+		static CopyPool pool;
+		return pool;
+	}
+
+	void copy(void *dst, const void *src, size_t n)
+	{
+		const size_t parts = n >= (size_t(2) << 20) ? workers_.size() + 1 : 1;
+		const size_t step = ((n + parts - 1) / parts + 63) & ~size_t(63);
+		Join join;
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			for (size_t off = step; off < n; off += step) {
+				tasks_.push_back(Task{static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
+					std::min(step, n - off), &join});
+				++join.left;
+			}
+		}
+		cv_.notify_all();
+		std::memcpy(dst, src, std::min(step, n));
+		std::unique_lock<std::mutex> lk(join.mu);
+		join.cv.wait(lk, [&] { return join.left == 0; });
+	}
+
+private:
+	struct Join {
+		std::mutex mu;
+		std::condition_variable cv;
+		size_t left = 0;
+	};
+	struct Task {
+		char *dst;
+		const char *src;
+		size_t n;
+		Join *join;
+	};
+
+	CopyPool()
+	{
+		const unsigned hw = std::thread::hardware_concurrency();
+		const unsigned n = hw > 1 ? std::min(hw - 1, 7u) : 0u;
+		for (unsigned i = 0; i < n; ++i)
+			workers_.emplace_back([this] { run(); });
+	}
+
+	~CopyPool()
+	{
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			stop_ = true;
+		}
+		cv_.notify_all();
+		for (std::thread &t : workers_)
+			t.join();
+	}
+
+	void run()
+	{
+		for (;;) {
+			Task t;
+			{
+				std::unique_lock<std::mutex> lk(mu_);
+				cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+				if (tasks_.empty())
+					return;
+				t = tasks_.front();
+				tasks_.pop_front();
+			}
+			std::memcpy(t.dst, t.src, t.n);
+			std::lock_guard<std::mutex> g(t.join->mu);
+			if (--t.join->left == 0)
+				t.join->cv.notify_all();
+		}
+	}
+
+	std::mutex mu_;
+	std::condition_variable cv_;
+	std::deque<Task> tasks_;
+	std::vector<std::thread> workers_;
+	bool stop_ = false;
+};
+
+// Host <-> device copies of the host entry point.  Page-locked caller memory
+// is copied by DMA directly.  Pageable memory (which the driver would stage
+// itself, one chunk at a time) goes through two pinned slots in chunks: the
+// host threads fill (or empty) one slot while the DMA engine moves the other.
+struct HostStage {
+	static constexpr size_t CHUNK = size_t(16) << 20;
+	PinBuf<unsigned char> slot[2];
+	cudaEvent_t ev[2] = {nullptr, nullptr};
+	bool busy[2] = {false, false}; // a DMA on the slot may still be in flight
+	int next = 0;
+
+	~HostStage()
+	{
+		for (cudaEvent_t e : ev)
+			if (e)
+				cudaEventDestroy(e);
+	}
+
+	static bool pinned(const void *p)
+	{
+		cudaPointerAttributes a;
+		if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+			cudaGetLastError();
+			return false;
+		}
+		return a.type == cudaMemoryTypeHost;
+	}
+
+	// A free slot: its last DMA has completed.
+	int take()
+	{
+		const int k = next;
+		next ^= 1;
+		if (!ev[k])
+			check(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+		slot[k].ensure(CHUNK);
+		if (busy[k])
+			check(cudaEventSynchronize(ev[k]));
+		busy[k] = false;
+		return k;
+	}
+
+	void in(void *dst, const void *src, size_t n, cudaStream_t s)
+	{
+		if (!n)
+			return;
+		if (pinned(src)) {
+			check(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s));
+			return;
+		}
+		for (size_t off = 0; off < n; off += CHUNK) {
+			const size_t len = std::min(CHUNK, n - off);
+			const int k = take();
+			CopyPool::get().copy(slot[k].p, static_cast<const char *>(src) + off, len);
+			check(cudaMemcpyAsync(static_cast<char *>(dst) + off, slot[k].p, len, cudaMemcpyHostToDevice, s));
+			check(cudaEventRecord(ev[k], s));
+			busy[k] = true;
+		}
+	}
+
+	// Returns with the copy complete.
+	void out(void *dst, const void *src, size_t n, cudaStream_t s)
+	{
+		if (!n)
+			return;
+		if (pinned(dst)) {
+			check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s));
+			check(cudaStreamSynchronize(s));
+			return;
+		}
+		const size_t nch = (n + CHUNK - 1) / CHUNK;
+		int k[2] = {-1, -1};
+		auto issue = [&](size_t i) {
+			const size_t off = i * CHUNK, len = std::min(CHUNK, n - off);
+			k[i & 1] = take();
+			check(cudaMemcpyAsync(slot[k[i & 1]].p, static_cast<const char *>(src) + off, len,
+				cudaMemcpyDeviceToHost, s));
+			check(cudaEventRecord(ev[k[i & 1]], s));
+			busy[k[i & 1]] = true;
+		};
+		issue(0);
+		for (size_t i = 0; i < nch; ++i) {
+			if (i + 1 < nch)
+				issue(i + 1);
+			const int ki = k[i & 1];
+			check(cudaEventSynchronize(ev[ki]));
+			busy[ki] = false;
+			const size_t off = i * CHUNK;
+			CopyPool::get().copy(static_cast<char *>(dst) + off, slot[ki].p, std::min(CHUNK, n - off));
+		}
 	}
 };
 
@@ -179,6 +363,7 @@ struct Workspace {
 	// Host-API staging of inputs and outputs.
 	DevBuf<double> hdata, herror, hgain, hrn, hbg, hclean;
 	DevBuf<uint8_t> hmask, hout;
+	HostStage stage_io; // pageable host buffers of the host entry point
 	DevBuf<unsigned> hflags; // failed map checks of the host entry point
 };
 
@@ -743,14 +928,14 @@ extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, d
 		ws->hclean.ensure(n);
 		ws->hout.ensure(n);
 		cudaStream_t s = nullptr;
-		check(cudaMemcpyAsync(ws->hdata.p, im->data, n * sizeof(double), cudaMemcpyHostToDevice, s));
+		ws->stage_io.in(ws->hdata.p, im->data, n * sizeof(double), s);
 		cusmic_image gpu = *im;
 		gpu.data = ws->hdata.p;
 		auto stage = [&](DevBuf<double> &b, const double *src) -> const double * {
 			if (!src)
 				return nullptr;
 			b.ensure(n);
-			check(cudaMemcpyAsync(b.p, src, n * sizeof(double), cudaMemcpyHostToDevice, s));
+			ws->stage_io.in(b.p, src, n * sizeof(double), s);
 			return b.p;
 		};
 		gpu.error = stage(ws->herror, im->error);
@@ -759,7 +944,7 @@ extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, d
 		gpu.background = stage(ws->hbg, im->background);
 		if (im->mask) {
 			ws->hmask.ensure(n);
-			check(cudaMemcpyAsync(ws->hmask.p, im->mask, n, cudaMemcpyHostToDevice, s));
+			ws->stage_io.in(ws->hmask.p, im->mask, n, s);
 			gpu.mask = ws->hmask.p;
 		}
 		DeviceInfo di = device_info(dev);
@@ -796,8 +981,8 @@ extern "C" int remove_cosmics(const cusmic_image *im, const cusmic_options *o, d
 		if (bad & 8u)
 			throw InvalidArgument("background must be finite");
 		finish(*ws, 1, s);
-		check(cudaMemcpy(clean, ws->hclean.p, n * sizeof(double), cudaMemcpyDeviceToHost));
-		check(cudaMemcpy(mask, ws->hout.p, n, cudaMemcpyDeviceToHost));
+		ws->stage_io.out(clean, ws->hclean.p, n * sizeof(double), s);
+		ws->stage_io.out(mask, ws->hout.p, n, s);
 	}, msg, len);
 }
 

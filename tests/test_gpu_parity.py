@@ -460,3 +460,57 @@ def test_ragged_mixed_error_maps_and_noise_model(cuda, oracle, mode):
             f.update(gain=1.0 + 0.5 * i, readnoise=3.0 + i)
         frames.append(f)
     check_against_oracle(oracle, frames, dict(SETTINGS, border=mode, maxiter=5), ragged=True)
+
+
+@pytest.mark.parametrize("kw,message", [
+    (dict(error=np.array([[1.0, 0.0], [1.0, 1.0]])), "error must be positive"),
+    (dict(error=np.array([[1.0, np.inf], [1.0, 1.0]])), "error must be finite"),
+    (dict(error=np.array([[np.nan, 0.0], [1.0, 1.0]]), background=np.nan), "error must be finite"),
+    (dict(effective_gain=-1.0, readnoise=1.0), "effective_gain must be positive"),
+    (dict(effective_gain=np.array([[1.0, 2.0], [np.inf, 1.0]]), readnoise=-1.0),
+     "effective_gain must be finite"),
+    (dict(effective_gain=1.0, readnoise=np.array([[0.0, -1.0], [0.0, 0.0]])),
+     "readnoise must be nonnegative"),
+    (dict(effective_gain=1.0, readnoise=1.0, background=np.array([[1.0, np.nan], [1.0, 1.0]])),
+     "background must be finite"),
+])
+def test_image_map_validation(cuda, kw, message):
+    """Python Image checks every map's contents on the device and reads them
+    back at once; the first failing check, in field order, raises the
+    reference's error (mod/cusmic/image.py:60-65)."""
+    from cusmic_b200 import Image
+    with pytest.raises(ValueError, match=message):
+        Image(np.ones((2, 2)), **kw)
+    Image(np.ones((2, 2)), effective_gain=2.0, readnoise=1.0, background=0.5)
+
+
+def test_host_api_pageable_and_pinned_buffers(cuda):
+    """The host entry point copies page-locked buffers by DMA and pageable ones
+    through pinned staging chunks (16 MiB, filled by host threads); both give
+    the same bits.  The frame spans two chunks per float64 plane."""
+    import torch
+    h, w = 1100, 2048
+    data, mask = small_scene(4242, h, w, holes=0.001, masked=0.005)
+    error = np.sqrt(np.abs(np.nan_to_num(data)) + 9)
+    o = cabi.options(**SETTINGS)
+    outs = []
+    for pinned in (False, True):
+        if pinned:
+            pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            d, e, m = pin(data), pin(error), pin(mask.astype(np.uint8))
+            c = torch.full((h, w), 7.0, dtype=torch.float64).pin_memory()
+            f = torch.full((h, w), 7, dtype=torch.uint8).pin_memory()
+            ptrs = (d.data_ptr(), e.data_ptr(), m.data_ptr(), c.data_ptr(), f.data_ptr())
+        else:
+            d, e, m = (np.ascontiguousarray(a) for a in (data, error, mask.astype(np.uint8)))
+            c, f = np.full((h, w), 7.0), np.full((h, w), 7, np.uint8)
+            ptrs = (d.ctypes.data, e.ctypes.data, m.ctypes.data, c.ctypes.data, f.ctypes.data)
+        im = cabi._native.Image(ptrs[0], ptrs[1], None, None, None, ptrs[2], w, h)
+        msg = ctypes.create_string_buffer(256)
+        st = cabi._native.lib().remove_cosmics(ctypes.byref(im), ctypes.byref(o), ptrs[3], ptrs[4],
+                                               msg, 256)
+        assert st == 0, msg.value
+        outs.append((np.array(c).copy(), np.array(f).copy()))
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    assert_bits_equal(outs[0][0], outs[1][0])
+    assert outs[0][1].any()
