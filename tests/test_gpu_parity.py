@@ -519,3 +519,34 @@ def test_host_api_pageable_and_pinned_buffers(cuda):
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
     assert_bits_equal(outs[0][0], outs[1][0])
     assert outs[0][1].any()
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_seeded_random_scenes(cuda, oracle, seed):
+    """Seeded random scenes against the oracle: sizes, border modes,
+    thresholds, pass counts, error map or noise model, holes, masks and
+    backgrounds all drawn from the seed."""
+    rng = np.random.default_rng(90000 + seed)
+    h, w = int(rng.integers(3, 130)), int(rng.integers(3, 130))
+    data = clustered_scene(int(rng.integers(1 << 30)), h, w) if rng.random() < 0.5 else \
+        small_scene(int(rng.integers(1 << 30)), h, w, rays=max(1, h * w // int(rng.integers(20, 200))))[0]
+    if rng.random() < 0.4:
+        data[rng.random((h, w)) < rng.uniform(0, 0.03)] = np.nan
+    frame = dict(data=data)
+    if rng.random() < 0.4:
+        frame["mask"] = rng.random((h, w)) < rng.uniform(0, 0.2)
+    if rng.random() < 0.3:
+        frame["background"] = rng.uniform(0, 50, (h, w)) if rng.random() < 0.5 else float(rng.uniform(0, 50))
+    cr = float(rng.uniform(2, 8))
+    opts = dict(contrast=float(rng.uniform(0.5, 5)), cr_threshold=cr,
+                neighbor_threshold=float(rng.uniform(0.5, cr)), maxiter=int(rng.integers(1, 9)),
+                border=MODES[int(rng.integers(len(MODES)))])
+    if rng.random() < 0.5:
+        frame["error"] = np.sqrt(np.abs(np.nan_to_num(data)) * rng.uniform(0.3, 1.0) + 9)
+    else:
+        g, r = float(rng.uniform(0.8, 3)), float(rng.uniform(1, 8))
+        frame.update(gain=g, readnoise=r)
+        opts.update(gain=g, readnoise=r)
+    if isinstance(frame.get("background"), float):
+        opts["background"] = frame["background"]
+    check_against_oracle(oracle, [frame], opts)
