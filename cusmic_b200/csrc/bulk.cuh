@@ -759,7 +759,7 @@ __device__ __forceinline__ void classify_flush(ClassifyStage &H, ClassifyStage &
 // consumer-warp region of an item, one lane per entry.  The high list grows
 // from the front of the candidate buffer, the low list from its back; a NaN
 // goes to the high list (the candidate kernel decides).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const int4 *__restrict__ items, int nitems, const PreCand *__restrict__ pre,
 	const int *__restrict__ pre_counts, DetectParams prm, Control *ctl, uint2 *cands)
