@@ -306,7 +306,7 @@ __device__ __forceinline__ unsigned long long dilate_row(unsigned long long e)
 // incremental pass lists the rows within six of a pixel whose value the last
 // replacement changed, and marks them.  A visited row's CHG bits and mark are
 // cleared (every row with a CHG bit is visited).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
 grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
 	const int2 *__restrict__ rows, int nrows, const int *dev_nrows, uint2 *targets, Control *ctl)
 {
