@@ -260,7 +260,7 @@ __device__ __forceinline__ NearMasks near_changed(const FrameDesc &fd, int y, in
 //    within 6 to the low list (back).
 // A row's classes are all this needs from the pass, so no other row waits.
 template <bool MODEL>
-__global__ void __launch_bounds__(256, MODEL ? 3 : 4)
+__global__ void __launch_bounds__(256, 4)
 incremental_rows_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ rows,
 	const int *nrows, DetectParams prm, Control *ctl, uint2 *cands)
 {
