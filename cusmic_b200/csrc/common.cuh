@@ -34,8 +34,9 @@ enum Plane {
 	P_EXCL,   // excluded from seeds and donors: hole or masked
 	P_DONOR,  // static donor: not excluded and finite after background
 	P_CRMASK, // cumulative cosmic-ray mask
-	P_HIGH,   // sig_raw > cr_threshold (or NaN) on the current clean pixels
-	P_LOW,    // neighbor_threshold < sig_raw, not HIGH
+	P_HIGH,   // holds every pixel with sig_raw > cr_threshold (or NaN) on the
+	          // current clean pixels (a superset after the first pass)
+	P_LOW,    // with HIGH, holds every pixel with sig_raw > neighbor_threshold
 	P_S1,     // significance > cr_threshold
 	P_S2,     // significance > neighbor_threshold
 	P_CAND,   // seed: S1, not excluded, contrast test passed

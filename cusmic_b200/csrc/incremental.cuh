@@ -21,8 +21,9 @@
 //
 //  * dirty_rows_kernel: the rows within 6 of D (the dirty rows), listed;
 //  * incremental_rows_kernel, per dirty row: sig_raw of every pixel within 2
-//    of D, which updates the HIGH / LOW class planes (classify_kernel's exact
-//    classes: sig_raw > cr_threshold or NaN, else > neighbor_threshold); a
+//    of D, which updates the HIGH / LOW class planes (exact classes: sig_raw
+//    > cr_threshold or NaN, else > neighbor_threshold; classify_kernel's
+//    first-pass classes are supersets, from the Laplacian upper bound); a
 //    pixel leaving HIGH loses its S1 and CAND bits (sig <= sig_raw <=
 //    cr_threshold), a pixel leaving both classes its S2 bit; then the HIGH
 //    pixels within 4 of D into the high list, the LOW pixels within 6 of D
@@ -36,8 +37,9 @@
 // marks before the replacement writes the next D.  What stays exact: S1 and CAND
 // everywhere, S2 of every HIGH pixel and of every LOW pixel with a CAND pixel
 // within 2 (the only S2 bits growth reads): a LOW pixel whose CAND
-// neighbourhood changed is within 6 of D.  A pixel outside both classes has
-// sig <= neighbor_threshold, so its bits are zero.
+// neighbourhood changed is within 6 of D.  Outside HIGH sig <= cr_threshold,
+// and a pixel outside both classes has sig <= neighbor_threshold, so its bits
+// are zero.
 #pragma once
 
 #include "bulk.cuh"
