@@ -550,3 +550,44 @@ def test_seeded_random_scenes(cuda, oracle, seed):
     if isinstance(frame.get("background"), float):
         opts["background"] = frame["background"]
     check_against_oracle(oracle, [frame], opts)
+
+
+def test_host_api_concurrent_calls(cuda):
+    """Host entry point calls from several threads at once (each call leases
+    its own workspace; the staging threads are shared) give the same bits as
+    the same calls one at a time."""
+    import threading
+    h, w = 700, 1500
+    frames = []
+    for i in range(4):
+        rng = np.random.default_rng(700 + i)
+        data = 100 + rng.normal(0, 10, (h, w))
+        ys, xs = rng.integers(0, h, 800), rng.integers(0, w, 800)
+        data[ys, xs] += rng.uniform(200, 5000, ys.size)
+        frames.append((data, np.sqrt(np.abs(data) + 9)))
+    o = cabi.options(**SETTINGS)
+
+    def clean(data, error):
+        out, flags = np.empty((h, w)), np.empty((h, w), np.uint8)
+        im = cabi._native.Image(data.ctypes.data, error.ctypes.data, None, None, None, None, w, h)
+        msg = ctypes.create_string_buffer(256)
+        st = cabi._native.lib().remove_cosmics(ctypes.byref(im), ctypes.byref(o), out.ctypes.data,
+                                               flags.ctypes.data, msg, 256)
+        assert st == 0, msg.value
+        return out, flags
+
+    want = [clean(*f) for f in frames]
+    got = [None] * len(frames)
+
+    def work(i):
+        got[i] = clean(*frames[i])
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(len(frames))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for (wc, wf), g in zip(want, got):
+        assert g is not None
+        np.testing.assert_array_equal(g[1], wf)
+        assert_bits_equal(g[0], wc)
