@@ -47,7 +47,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Mpix/s (f64, maxiter=4, identical masks) batched vs plain; bwd/fwd time"
 SETTINGS = dict(contrast=3.0, cr_threshold=5.0, neighbor_threshold=3.0, maxiter=4)
-SIG_BULK_DRAM_BYTES_PER_PX = 8.86  # ncu: 148.7 MB per launch over 16.78 Mpix
+SIG_BULK_DRAM_BYTES_PER_PX = 8.62  # ncu: 144.6 MB per launch over 16.78 Mpix
 
 
 def parse_args():
