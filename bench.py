@@ -230,13 +230,13 @@ def main():
     kms = {k: sum(p[0][k] for p in prof) / len(prof) for k in kinds}
     klaunch = {k: prof[0][1][k] for k in kinds}
     # Dense detection kernel (sig_bulk_kernel), run by the first (full) pass
-    # over every frame; its event span also holds the zeroing of the S1, S2,
-    # CAND and FRESH planes before it.  Per pixel: read clean (8 B), zero four
-    # bit planes (4/8 B).  The error map is not read there: its 32 x 32 block
+    # over every frame.  Per pixel it reads clean (8 B); its bit planes were
+    # zeroed by the call's prologue memset, and its writes (the sparse pre
+    # list) are a few MB.  The error map is not read there: its 32 x 32 block
     # floors are computed once per call by floor_kernel.  Later passes are
     # incremental and do not run it.
     active_px = nf * h * w * klaunch["sigraw"]
-    detect_bytes = active_px * (8 + 4 / 8)
+    detect_bytes = active_px * 8
     detect_ms = kms["sigraw"]
     achieved = detect_bytes / (detect_ms / 1e3) / 1e9
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
@@ -254,10 +254,11 @@ def main():
                 "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4),
                 "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
                 "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
-    # Kernels of one execution as the event profiler saw them, plus two per
-    # pass that share a mark with another kernel: the plane zeroing that starts
-    # every pass (full or incremental) and the replacement's target selection.
-    launches_per_step = sum(klaunch.values()) + 2 * (klaunch["sigraw"] + klaunch["dirty"])
+    # Kernels of one execution as the event profiler saw them, plus those that
+    # share a mark with another kernel: the replacement's target selection
+    # (every pass) and the FRESH-plane zeroing that starts each incremental
+    # pass.
+    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"] + 2 * klaunch["dirty"]
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),

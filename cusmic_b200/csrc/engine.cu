@@ -692,19 +692,15 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	const int nbulk = (int)L.bulk.size();
 	const int cap = di.sms * L.tune.dense_blocks_per_sm, sparse = di.sms * L.tune.sparse_blocks_per_sm;
 	const int rowb = L.tune.row_blocks_per_sm;
-	{
-		// Full: S1, S2, CAND and FRESH of every frame (contiguous planes) and
-		// the growth row marks; incremental: FRESH (its growth visits a row
-		// list).  In 16-byte words.
-		const int first = incremental ? P_FRESH : P_S1, planes = incremental ? 1 : 4;
-		const long long n16 = planes * L.plane_words / 4, m16 = incremental ? 0 : L.row_words / 4;
-		const long long blocks = (n16 + m16 + 255) / 256 < di.sms * 4 ? (n16 + m16 + 255) / 256
-		                                                              : di.sms * 4;
-		zero_words_kernel<<<(int)blocks, 256, 0, s>>>(
-			reinterpret_cast<uint4 *>(ws.bits.p + first * L.plane_words), n16,
-			reinterpret_cast<uint4 *>(ws.rowmarks.p), m16);
-	}
 	if (incremental) {
+		// FRESH of every frame (its growth visits a row list); the full pass
+		// finds S1, S2, CAND, FRESH and the growth row marks zeroed by the
+		// prologue.  In 16-byte words.
+		const long long n16 = L.plane_words / 4;
+		const long long blocks = (n16 + 255) / 256 < di.sms * 4 ? (n16 + 255) / 256 : di.sms * 4;
+		zero_words_kernel<<<(int)blocks, 256, 0, s>>>(
+			reinterpret_cast<uint4 *>(ws.bits.p + P_FRESH * L.plane_words), n16,
+			reinterpret_cast<uint4 *>(ws.rowmarks.p), 0);
 		const int tb = (nrows + 255) / 256 < di.sms * 4 ? (nrows + 255) / 256 : di.sms * 4;
 		dirty_rows_kernel<<<tb, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows, L.prm.mode,
 			ws.ctl.p, ws.dirty.p);
@@ -775,8 +771,12 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		mark(rec, K_COPY);
 		return;
 	}
-	// Zero bit planes (prepare_kernel writes HOLE, EXCL and DONOR) and row marks.
-	check(cudaMemsetAsync(ws.bits.p, 0, (size_t)L.total_words * sizeof(uint32_t), s));
+	// Zero the bit planes after DONOR (prepare_kernel writes every word of
+	// HOLE, EXCL and DONOR) and both row-mark arrays: nothing else writes them
+	// before the first pass, which therefore clears nothing itself.
+	static_assert(P_HOLE == 0 && P_EXCL == 1 && P_DONOR == 2 && P_CRMASK == 3, "plane order");
+	check(cudaMemsetAsync(ws.bits.p + P_CRMASK * L.plane_words, 0,
+		(size_t)(N_PLANES - P_CRMASK) * L.plane_words * sizeof(uint32_t), s));
 	check(cudaMemsetAsync(ws.rowmarks.p, 0, 2 * (size_t)L.row_words * sizeof(uint32_t), s));
 	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
 		nrows, ws.ctl.p, ws.cands.p);
