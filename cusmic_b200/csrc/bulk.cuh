@@ -23,7 +23,7 @@
 //    below, and the model evaluated at it with the block's gain and read noise
 //    bounds the noise from below: the model is non-decreasing in the median
 //    and in the read noise and non-increasing in the gain;
-//  * sig_bulk_kernel (every pass): the Laplacian of every pixel against T of
+//  * sig_bulk_kernel (the full first pass): the Laplacian of every pixel against T of
 //    its block.  Every pixel whose sig_raw exceeds min(cr, nb) passes (the
 //    product is rounded by at most 2^-53 relative, the margin is 1e-12 and
 //    the upper bound of the Laplacian used here is never below the
@@ -46,7 +46,7 @@
 // shift).  Each ring row has a "full" mbarrier (lane 0's transaction bytes
 // plus lane 1's cp.async arrive) and an "empty" mbarrier on which each of the
 // four consumer warps arrives when it is done with the row.  (The S1, S2 and
-// CAND planes are zeroed before the pass by zero_words_kernel.)  A block takes items
+// CAND planes were zeroed by the call's prologue memset.)  A block takes items
 // of BK_COLS x BK_ROWS pixels from a ticket counter (items of frames that
 // stopped are skipped there) and the ring runs straight through from one item
 // into the next.
@@ -631,12 +631,15 @@ __device__ __forceinline__ bool bulk_consumer(BulkRing &R, const FrameDesc *__re
 			}
 			ql = n[0] * 0.25;
 			qr = n[5] * 0.25;
+			bool pass[4];
 #pragma unroll
-			for (int i = 0; i < 4; ++i) {
-				const bool pass = hi_word(lap[i]) >= thr[i];
-				const unsigned bal = __ballot_sync(0xffffffffu, pass);
-				if (bal) {
-					if (pass)
+			for (int i = 0; i < 4; ++i)
+				pass[i] = hi_word(lap[i]) >= thr[i];
+			if (__any_sync(0xffffffffu, pass[0] | pass[1] | pass[2] | pass[3])) {
+#pragma unroll
+				for (int i = 0; i < 4; ++i) {
+					const unsigned bal = __ballot_sync(0xffffffffu, pass[i]);
+					if (pass[i])
 						region[cnt + __popc(bal & below)] =
 							PreCand{(unsigned)(pix0 + i), (unsigned)f, lap[i]};
 					cnt += __popc(bal);
