@@ -114,15 +114,29 @@ def dist_setup(args):
     return world, rank, local
 
 
-def cpu_reference(frame, error, mask, rows):
-    """Time the CPU oracle on the first `rows` rows of one frame (all threads)."""
+def cpu_reference(frame, error, mask, rows, threads=0):
+    """Time the CPU oracle on the first `rows` rows of one frame (all host
+    threads, or `threads` of them)."""
     from oracle import oracle
     sub = np.ascontiguousarray(frame[:rows])
-    t = time.perf_counter()
-    oracle.clean_frame(sub, error=np.ascontiguousarray(error[:rows]),
-                       mask=np.ascontiguousarray(mask[:rows]), border="mirror", **SETTINGS)
-    dt = time.perf_counter() - t
+    prev = oracle.set_threads(0)
+    oracle.set_threads(threads or os.cpu_count())
+    try:
+        t = time.perf_counter()
+        oracle.clean_frame(sub, error=np.ascontiguousarray(error[:rows]),
+                           mask=np.ascontiguousarray(mask[:rows]), border="mirror", **SETTINGS)
+        dt = time.perf_counter() - t
+    finally:
+        oracle.set_threads(prev)
     return sub.size / dt / 1e6, dt, sub.size
+
+
+def cpu_single_thread(frame, error, mask, rows):
+    """The CPU oracle on one host thread (a like-for-like stand-in for a
+    single-threaded CPU implementation), on an eighth of the sample rows."""
+    v, dt, n = cpu_reference(frame, error, mask, max(32, rows // 8), threads=1)
+    return {"value": round(v, 4), "unit": "Mpix/s", "cores": 1,
+            "sample": f"{n // frame.shape[1]}x{frame.shape[1]} rows of frame 0 ({n} px, {dt:.1f} s)"}
 
 
 def run_reference_arm(args, world, rank):
@@ -151,7 +165,9 @@ def run_reference_arm(args, world, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args),
         "cpu_baseline": {"value": round(value, 4), "unit": "Mpix/s", "cores": cores,
-                         "kind": "port", "sample": sample},
+                         "kind": "port", "sample": sample,
+                         "single_thread": cpu_single_thread(f.data, sc.error, sc.mask,
+                                                            args.cpu_sample_rows)},
         "e2e": {"value": round(value, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -318,7 +334,9 @@ def main():
         out["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpix/s", "cores": os.cpu_count(),
                                "kind": "port",
                                "sample": f"{args.cpu_sample_rows}x{w} rows of frame 0 "
-                                         f"({n} px, {dt:.1f} s), maxiter=4, OpenMP threads"}
+                                         f"({n} px, {dt:.1f} s), maxiter=4, OpenMP threads",
+                               "single_thread": cpu_single_thread(
+                                   sc.frames[0].data, sc.error, sc.mask, args.cpu_sample_rows)}
         print(json.dumps(out))
     plan.close()
     if world > 1:

@@ -759,6 +759,24 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	mark(rec, K_REPLACE);
 }
 
+// prepare_kernel: one compiled for noise-model frames without maps, with
+// twice the unroll, when every frame is of that kind; otherwise the kernel
+// that decides per row (faster for error-map frames than any specialisation
+// that was timed).
+static void launch_prepare(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s)
+{
+	bool model = true;
+	for (const FrameDesc &fd : L.frames)
+		model = model && prep_kind(fd) == PREP_MODEL;
+	const int nrows = (int)L.rows.size(), grid = grid_for_rows(di, nrows, L.tune.row_blocks_per_sm);
+	if (model)
+		prepare_kernel<PREP_MODEL, 2 * ROW_UNROLL><<<grid, 256, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
+	else
+		prepare_kernel<PREP_ANY><<<grid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows,
+			ws.ctl.p, ws.cands.p);
+}
+
 static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
 	Recorder *rec = nullptr)
 {
@@ -778,8 +796,7 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	check(cudaMemsetAsync(ws.bits.p + P_CRMASK * L.plane_words, 0,
 		(size_t)(N_PLANES - P_CRMASK) * L.plane_words * sizeof(uint32_t), s));
 	check(cudaMemsetAsync(ws.rowmarks.p, 0, 2 * (size_t)L.row_words * sizeof(uint32_t), s));
-	prepare_kernel<<<grid_for_rows(di, nrows, L.tune.row_blocks_per_sm), 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p,
-		nrows, ws.ctl.p, ws.cands.p);
+	launch_prepare(ws, L, di, s);
 	mark(rec, K_PREPARE);
 	// Block floors: error-map thresholds; noise-model keys from prepare's row
 	// minima of the non-hole pixels, which the hole fill and every later
@@ -1495,7 +1512,7 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 			// Bit planes start at zero (prepare_kernel writes HOLE, EXCL and
 			// DONOR); the scratch keeps the previous call's contents.
 			check(cudaMemsetAsync(fd.bits, 0, (size_t)N_PLANES * L.plane * sizeof(uint32_t), s));
-			prepare_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h);
+			prepare_kernel<PREP_ANY><<<row_blocks, 256, 0, s>>>(frames, state, rows, h);
 			fill_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h);
 			for (int it = 0; it < o->maxiter; ++it) {
 				if (error_map) {

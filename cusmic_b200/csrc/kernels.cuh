@@ -136,11 +136,25 @@ __device__ __forceinline__ double order_value(unsigned long long k)
 // in flight per SM to approach the HBM bandwidth.
 constexpr int ROW_UNROLL = 4;
 
+// Frame kinds of prepare_row: the input maps it reads and whether it writes
+// noise-model row minima.  A batch whose frames are all of one kind gets a
+// prepare_kernel compiled for that kind (PREP_ANY decides per row).
+enum PrepKind { PREP_ANY, PREP_PLAIN, PREP_MASK, PREP_MAPS, PREP_MODEL, PREP_MODEL_MAPS };
+
+CB_HD int prep_kind(const FrameDesc &fd)
+{
+	const bool mask = fd.mask, bgmap = fd.bg_map;
+	if (fd.floors && !fd.error) // noise-model frame: row minima for the floors
+		return mask || bgmap ? PREP_MODEL_MAPS : PREP_MODEL;
+	return bgmap ? PREP_MAPS : mask ? PREP_MASK : PREP_PLAIN;
+}
+
+
 // One row of prepare_kernel for the frame kinds that occur: MASK = input
 // mask, BGMAP = background map.  Descriptor fields are held in registers (the
 // stores below go through pointers the compiler cannot prove distinct from
 // them).
-template <bool MASK, bool BGMAP, bool ROWMIN>
+template <bool MASK, bool BGMAP, bool ROWMIN, int U = ROW_UNROLL>
 __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st, int f, int y,
 	Control *ctl, uint2 *holes)
 {
@@ -164,14 +178,14 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 	uint32_t *rowmin = ROWMIN ? plane_ptr(fd, P_ROWMIN) + roww : nullptr;
 	for (int seg = 0; seg * 1024 < w; ++seg) {
 		uint32_t my_h = 0, my_e = 0, my_d = 0, my_m = 0xffffffffu;
-		for (int c0 = 0; c0 < 32; c0 += ROW_UNROLL) {
+		for (int c0 = 0; c0 < 32; c0 += U) {
 			const int xb = seg * 1024 + c0 * 32;
 			if (xb >= w)
 				break; // warp-uniform
-			double d[ROW_UNROLL], bg[ROW_UNROLL];
-			bool m[ROW_UNROLL];
+			double d[U], bg[U];
+			bool m[U];
 #pragma unroll
-			for (int u = 0; u < ROW_UNROLL; ++u) {
+			for (int u = 0; u < U; ++u) {
 				const int x = xb + 32 * u + lane;
 				d[u] = 0;
 				bg[u] = bgv;
@@ -185,7 +199,7 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 				}
 			}
 #pragma unroll
-			for (int u = 0; u < ROW_UNROLL; ++u) {
+			for (int u = 0; u < U; ++u) {
 				const int x0 = xb + 32 * u;
 				const int x = x0 + lane;
 				const bool valid = x < w;
@@ -250,6 +264,8 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 // segment's word j, so each plane gets one coalesced store per segment.  The
 // other planes were zeroed before the kernel.  Holes are not listed: the hole
 // fill scans the HOLE plane.
+// UL: the unroll of the kinds without maps.
+template <int KIND = PREP_ANY, int UL = ROW_UNROLL>
 __global__ void __launch_bounds__(256, 4)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
 	int nrows, Control *ctl = nullptr, uint2 *holes = nullptr)
@@ -259,17 +275,20 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 		const int2 item = rows[r];
 		const FrameDesc &fd = frames[item.x];
 		FrameState &st = state[item.x];
-		const bool mask = fd.mask, bgmap = fd.bg_map;
-		if (fd.floors && !fd.error) { // noise-model frame: row minima for the floors
-			if (!mask && !bgmap)
-				prepare_row<false, false, true>(fd, st, item.x, item.y, ctl, holes);
-			else
-				prepare_row<true, true, true>(fd, st, item.x, item.y, ctl, holes);
-		} else if (mask && !bgmap) {
-			prepare_row<true, false, false>(fd, st, item.x, item.y, ctl, holes);
-		} else if (!mask && !bgmap) {
-			prepare_row<false, false, false>(fd, st, item.x, item.y, ctl, holes);
-		} else {
+		switch (KIND == PREP_ANY ? prep_kind(fd) : KIND) {
+		case PREP_MODEL:
+			prepare_row<false, false, true, UL>(fd, st, item.x, item.y, ctl, holes);
+			break;
+		case PREP_MODEL_MAPS:
+			prepare_row<true, true, true>(fd, st, item.x, item.y, ctl, holes);
+			break;
+		case PREP_MASK:
+			prepare_row<true, false, false, UL>(fd, st, item.x, item.y, ctl, holes);
+			break;
+		case PREP_PLAIN:
+			prepare_row<false, false, false, UL>(fd, st, item.x, item.y, ctl, holes);
+			break;
+		default:
 			prepare_row<true, true, false>(fd, st, item.x, item.y, ctl, holes);
 		}
 	}

@@ -21,6 +21,9 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 enum { O_REFLECT, O_CONSTANT, O_NEAREST, O_MIRROR, O_WRAP };
 
@@ -560,4 +563,20 @@ oracle_backward(const oracle_image *im, const oracle_options *o, const uint8_t *
 	free(donor);
 	free(keys);
 	free(idx);
+}
+
+/* Host threads of the OpenMP loops above (n <= 0: leave as is); returns the
+ * count in effect.  The CPU baseline times the restatement both on one thread
+ * and on every host core. */
+int
+oracle_set_threads(int n)
+{
+#ifdef _OPENMP
+	if (n > 0)
+		omp_set_num_threads(n);
+	return omp_get_max_threads();
+#else
+	(void)n;
+	return 1;
+#endif
 }

@@ -59,7 +59,14 @@ def lib():
                                             ctypes.c_int, ctypes.c_int]
         _lib.oracle_laplacian.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _lib.oracle_replace.argtypes = [_dp, _bp, _bp, ctypes.c_int, ctypes.c_int]
+        _lib.oracle_set_threads.restype = ctypes.c_int
+        _lib.oracle_set_threads.argtypes = [ctypes.c_int]
     return _lib
+
+
+def set_threads(n):
+    """Host threads of the oracle's OpenMP loops (0: unchanged); returns the count in effect."""
+    return lib().oracle_set_threads(int(n))
 
 
 def _f64(a):

@@ -183,3 +183,19 @@ def test_no_donors_is_an_error(oracle):
     mask[3, 3] = False
     with pytest.raises(oracle.OracleError, match="no finite replacement donors"):
         oracle.clean_frame(data, error=np.ones_like(data), mask=mask, **SETTINGS)
+
+
+def test_thread_count_does_not_change_results(oracle, golden):
+    """The CPU baseline times the oracle on one thread and on every core: both
+    must compute the same bits."""
+    data, err = golden["data"][:160], golden["error"][:160]
+    prev = oracle.set_threads(0)
+    try:
+        out = []
+        for n in (1, max(2, prev)):
+            assert oracle.set_threads(n) == n
+            out.append(oracle.clean_frame(data, error=err, **golden["settings"]))
+    finally:
+        oracle.set_threads(prev)
+    assert_bits_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
