@@ -430,6 +430,30 @@ def ragged_comparison(dev, stream, barrier):
             "identical_masks": bool(same), "kernel_ms": kernel_ms}
 
 
+# Cycles of the sleep kernel ahead of a gated interval (about 0.27 ms at
+# 1.965 GHz): longer than the host's overhead for one call.
+GATE_CYCLES = 1 << 19
+
+
+def gated_ms(stream, call):
+    """CUDA-event time of call() on `stream`.  A short sleep kernel ahead of the
+    start event holds the stream while the host runs the call's Python and C
+    checks, so the interval starts with the call's device work.  A call that
+    synchronises on entry must get a stream other than the one its last
+    execution ran on (the backward, after a forward on another stream); for a
+    call that synchronises before returning (the backward) the interval ends
+    with the host's return from that wait."""
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(GATE_CYCLES)
+    s.record(stream)
+    out = call()
+    e.record(stream)
+    e.synchronize()
+    return s.elapsed_time(e), out
+
+
 def large_run(dev, stream, barrier):
     """large_8192: forward and frozen-mask backward of 4 x 8192^2 float64 frames
     (full-size error map, 2% mask), with the device memory the process holds."""
@@ -452,21 +476,14 @@ def large_run(dev, stream, barrier):
     torch.cuda.synchronize(dev)
     reps = 3
     fwd = bwd = 0.0
+    side = torch.cuda.Stream(device=dev)
     for _ in range(reps):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
-        s.record(stream)
-        plan.execute(stream)
-        e.record(stream)
+        t, _ = gated_ms(stream, lambda: plan.execute(stream))
         plan.wait()
-        fwd += s.elapsed_time(e)
-        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s2.record(stream)
-        gx, _ = plan.backward(g, stream)
-        e2.record(stream)
-        torch.cuda.synchronize(dev)
-        bwd += s2.elapsed_time(e2)
-        del gx
+        fwd += t
+        t, _ = gated_ms(side, lambda: plan.backward(g, side))
+        bwd += t
     free1, _ = torch.cuda.mem_get_info(dev)
     px = stack.numel()
     out = {"workload": "large_8192: 4 x 8192x8192 float64, full error map, 2% mask, 3000 rays "
@@ -501,20 +518,14 @@ def adjoint_timing(dev, stream, barrier):
         plan.backward(g, stream)
     reps = 10
     fwd = bwd = 0.0
+    side = torch.cuda.Stream(device=dev)
     for _ in range(reps):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
-        s.record(stream)
-        plan.execute(stream)
-        e.record(stream)
+        t, _ = gated_ms(stream, lambda: plan.execute(stream))
         plan.wait()
-        fwd += s.elapsed_time(e)
-        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s2.record(stream)
-        plan.backward(g, stream)
-        e2.record(stream)
-        torch.cuda.synchronize(dev)
-        bwd += s2.elapsed_time(e2)
+        fwd += t
+        t, _ = gated_ms(side, lambda: plan.backward(g, side))
+        bwd += t
     plan.close()
     return {"workload": "adjoint_1024: 8 x 1024x1024, gain=2 rn=5 bg=0, L = sum(w * cleaned)",
             "fwd_ms": round(fwd / reps, 4), "bwd_ms": round(bwd / reps, 4),

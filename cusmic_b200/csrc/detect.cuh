@@ -405,9 +405,11 @@ __device__ __forceinline__ double warp_sort32(double v)
 	for (int span = 2; span <= 32; span *= 2) {
 #pragma unroll
 		for (int step = span / 2; step; step /= 2) {
-			double peer = __shfl_xor_sync(0xffffffffu, v, step);
-			bool lower = ((lane & span) == 0) == ((lane & step) == 0);
-			v = lower ? dmin(v, peer) : dmax(v, peer);
+			const double peer = __shfl_xor_sync(0xffffffffu, v, step);
+			const bool lower = ((lane & span) == 0) == ((lane & step) == 0);
+			// The lower lane keeps the smaller value, the upper the larger;
+			// on equal values either choice is the same value.
+			v = (peer < v) == lower ? peer : v;
 		}
 	}
 	return v;
@@ -613,31 +615,35 @@ candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restri
 	}
 }
 
-// Element `rank` of the 64 values held as (a, b) = slots (lane, 32 + lane) of a
-// warp, by an ascending bitonic network.  NaN-free inputs.
-__device__ __forceinline__ double warp_rank64(double a, double b, int rank)
+// Element RANK < 32 of the 64 values held as (a, b) = slots (lane, 32 + lane)
+// of a warp, by an ascending bitonic network: a sorts ascending and b
+// descending, the half-cleaner keeps the 32 smallest in a, and only a is
+// merged further.  NaN-free inputs; on equal values either choice of a
+// compare-exchange is the same value.
+template <int RANK>
+__device__ __forceinline__ double warp_rank64(double a, double b)
 {
+	static_assert(RANK >= 0 && RANK < 32, "the lower half holds the rank");
 	const int lane = threadIdx.x & 31;
 #pragma unroll
-	for (int k = 2; k <= 64; k <<= 1) {
+	for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
 		for (int j = k >> 1; j > 0; j >>= 1) {
-			if (j == 32) {
-				cas(a, b);
-			} else {
-				double pa = __shfl_xor_sync(0xffffffffu, a, j);
-				double pb = __shfl_xor_sync(0xffffffffu, b, j);
-				int ea = lane, eb = lane + 32;
-				bool mina = ((ea & j) == 0) == ((ea & k) == 0);
-				bool minb = ((eb & j) == 0) == ((eb & k) == 0);
-				a = mina ? dmin(a, pa) : dmax(a, pa);
-				b = minb ? dmin(b, pb) : dmax(b, pb);
-			}
+			const double pa = __shfl_xor_sync(0xffffffffu, a, j);
+			const double pb = __shfl_xor_sync(0xffffffffu, b, j);
+			const bool mina = ((lane & j) == 0) == ((lane & k) == 0);
+			const bool minb = ((lane & j) == 0) == (((lane + 32) & k) == 0);
+			a = (pa < a) == mina ? pa : a;
+			b = (pb < b) == minb ? pb : b;
 		}
 	}
-	double ra = __shfl_sync(0xffffffffu, a, rank & 31);
-	double rb = __shfl_sync(0xffffffffu, b, rank & 31);
-	return rank < 32 ? ra : rb;
+	a = dmin(a, b);
+#pragma unroll
+	for (int j = 16; j > 0; j >>= 1) {
+		const double pa = __shfl_xor_sync(0xffffffffu, a, j);
+		a = (pa < a) == ((lane & j) == 0) ? pa : a;
+	}
+	return __shfl_sync(0xffffffffu, a, RANK);
 }
 
 // The warp's fine-structure test of a seed at (x, y) (src/filters.cuh:148-175):
@@ -703,7 +709,7 @@ __device__ __forceinline__ void seed_eval(const FrameDesc &fd, int x, int y, dou
 		}
 	}
 	const double med3c = __shfl_sync(0xffffffffu, m3[0], 24);
-	const double med7 = warp_rank64(m3[0], m3[1], 24);
+	const double med7 = warp_rank64<24>(m3[0], m3[1]);
 	double fine = (med3c - med7) / noise;
 	fine = fine < FINE_FLOOR ? FINE_FLOOR : fine;
 	const bool cand = sig / fine > prm.contrast;
