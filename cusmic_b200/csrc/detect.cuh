@@ -589,11 +589,15 @@ candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restri
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)ctl->n_low;
 	const unsigned long long cap = ctl->cand_cap;
-	for (long long base = gw * 32; base < n; base += nw * 32) {
+	// Entries per warp and sweep: 32 for a long list; a short list (the late
+	// passes) is spread thinner so that its survivors, which a warp
+	// evaluates one after another, land on different warps.
+	const int chunk = n >= nw * 32 ? 32 : n > nw ? (int)((n + nw - 1) / nw) : 1;
+	for (long long base = gw * chunk; base < n; base += nw * chunk) {
 		const long long e = base + lane;
 		uint2 t = make_uint2(0, 0);
 		bool near = false;
-		if (e < n) {
+		if (lane < chunk && e < n) {
 			t = cands[cap - 1 - e];
 			const FrameDesc &fd = frames[t.x];
 			const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
