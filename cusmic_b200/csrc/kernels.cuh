@@ -767,32 +767,49 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 		const bool has_bg = fd.has_bg;
 		if (!has_bg) { // warp-uniform
 			// clean already holds the output: only the mask and the restored
-			// non-finite inputs are written, a lane per bit word (16-byte
-			// mask stores where the row's bytes are aligned).
+			// non-finite inputs are written.  Groups of 32 bit words (1024
+			// pixels), two groups' words loaded before either is used; a
+			// full group of an aligned row goes out as two contiguous
+			// 512-byte warp stores (lane j: the 16 pixels of half (j & 1) of
+			// word 16 q + j / 2), the rest byte by byte.
 			const bool vec = ((uintptr_t)mask_out & 15u) == 0;
-			for (int k = lane; k < words; k += 32) {
-				const uint32_t cbits = crm[k];
-				const int x0 = 32 * k, n = min(32, w - x0);
-				if (vec && n == 32) {
-					uint4 *dst = reinterpret_cast<uint4 *>(mask_out + x0);
+			for (int k0 = 0; k0 < words; k0 += 64) {
+				uint32_t cw[2], hw[2];
 #pragma unroll
-					for (int q = 0; q < 2; ++q) {
-						uint32_t v[4];
-#pragma unroll
-						for (int b = 0; b < 4; ++b) {
-							const uint32_t nib = cbits >> (16 * q + 4 * b);
-							v[b] = (nib & 1u) | ((nib >> 1) & 1u) << 8 | ((nib >> 2) & 1u) << 16 |
-							       ((nib >> 3) & 1u) << 24;
-						}
-						dst[q] = make_uint4(v[0], v[1], v[2], v[3]);
-					}
-				} else {
-					for (int i = 0; i < n; ++i)
-						mask_out[x0 + i] = (cbits >> i) & 1u;
+				for (int g = 0; g < 2; ++g) {
+					const int k = k0 + 32 * g + lane;
+					cw[g] = k < words ? crm[k] : 0u;
+					hw[g] = k < words ? hole[k] : 0u;
 				}
-				for (uint32_t hb = hole[k]; hb; hb &= hb - 1) {
-					const int x = x0 + __ffs(hb) - 1;
-					clean[x] = data[x];
+#pragma unroll
+				for (int g = 0; g < 2; ++g) {
+					const int kb = k0 + 32 * g, k = kb + lane;
+					if (kb >= words)
+						break; // warp-uniform
+					if (vec && 32 * (kb + 32) <= w) { // warp-uniform
+#pragma unroll
+						for (int q = 0; q < 2; ++q) {
+							const uint32_t word = __shfl_sync(0xffffffffu, cw[g], 16 * q + (lane >> 1));
+							const uint32_t half = word >> (16 * (lane & 1));
+							uint32_t v[4];
+#pragma unroll
+							for (int b = 0; b < 4; ++b) {
+								const uint32_t nib = half >> (4 * b);
+								v[b] = (nib & 1u) | ((nib >> 1) & 1u) << 8 | ((nib >> 2) & 1u) << 16 |
+								       ((nib >> 3) & 1u) << 24;
+							}
+							*reinterpret_cast<uint4 *>(mask_out + 32 * kb + 512 * q + 16 * lane) =
+								make_uint4(v[0], v[1], v[2], v[3]);
+						}
+					} else if (k < words) {
+						const int x0 = 32 * k, n = min(32, w - x0);
+						for (int i = 0; i < n; ++i)
+							mask_out[x0 + i] = (cw[g] >> i) & 1u;
+					}
+					for (uint32_t hb = hw[g]; hb; hb &= hb - 1) {
+						const int x = 32 * k + __ffs(hb) - 1;
+						clean[x] = data[x];
+					}
 				}
 			}
 			continue;
