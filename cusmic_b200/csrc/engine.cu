@@ -13,6 +13,7 @@
 #include "detect.cuh"
 #include "bulk.cuh"
 #include "kernels.cuh"
+#include "prepare_bulk.cuh"
 #include "incremental.cuh"
 #include "backward.cuh"
 
@@ -333,8 +334,13 @@ static DeviceInfo device_info(int dev)
 	if ((int)cache.size() <= dev)
 		cache.resize(dev + 1);
 	DeviceInfo &d = cache[dev];
-	if (!d.sms)
+	if (!d.sms) { // first use on this (the current) device
 		check(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+		check(cudaFuncSetAttribute(prepare_bulk_kernel<false>,
+			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
+		check(cudaFuncSetAttribute(prepare_bulk_kernel<true>,
+			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
+	}
 	return d;
 }
 
@@ -759,16 +765,32 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	mark(rec, K_REPLACE);
 }
 
-// prepare_kernel: one compiled for noise-model frames without maps, with
-// twice the unroll, when every frame is of that kind; otherwise the kernel
-// that decides per row (faster for error-map frames than any specialisation
-// that was timed).
+// prepare: the bulk-staged kernel when every frame suits it; else one
+// compiled for noise-model frames without maps, with twice the unroll, when
+// every frame is of that kind; otherwise the kernel that decides per row
+// (faster for error-map frames than any specialisation that was timed).
 static void launch_prepare(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s)
 {
-	bool model = true;
-	for (const FrameDesc &fd : L.frames)
-		model = model && prep_kind(fd) == PREP_MODEL;
-	const int nrows = (int)L.rows.size(), grid = grid_for_rows(di, nrows, L.tune.row_blocks_per_sm);
+	bool model = true, bulk = true, rowmin = false;
+	for (const FrameDesc &fd : L.frames) {
+		const int kind = prep_kind(fd);
+		model = model && kind == PREP_MODEL;
+		bulk = bulk && prep_bulk_ok(fd);
+		rowmin = rowmin || kind == PREP_MODEL || kind == PREP_MODEL_MAPS;
+	}
+	const int nrows = (int)L.rows.size();
+	if (bulk) {
+		const int need = (nrows + PB_WARPS - 1) / PB_WARPS, cap = di.sms * PB_BLOCKS;
+		const int grid = need < cap ? need : cap;
+		if (rowmin)
+			prepare_bulk_kernel<true><<<grid, 32 * PB_WARPS, PB_SMEM, s>>>(ws.frames.p, ws.state.p,
+				ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
+		else
+			prepare_bulk_kernel<false><<<grid, 32 * PB_WARPS, PB_SMEM, s>>>(ws.frames.p, ws.state.p,
+				ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
+		return;
+	}
+	const int grid = grid_for_rows(di, nrows, L.tune.row_blocks_per_sm);
 	if (model)
 		prepare_kernel<PREP_MODEL, 2 * ROW_UNROLL><<<grid, 256, 0, s>>>(ws.frames.p, ws.state.p,
 			ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
