@@ -14,8 +14,10 @@ pixels) are larger than the 126 MB L2, so no flush is needed between steps.
 * ``e2e``: the same metric through the reference-facing host entry point
   ``remove_cosmics`` (one call per frame, pinned host buffers in and out,
   every copy inside the timed region).
-* ``roofline``: the detection kernel's algorithmic bytes per launch over its
-  CUDA-event duration, against the measured HBM copy bandwidth.
+* ``roofline``: the dominant kernel (prepare, the largest share of kernel
+  time): its algorithmic bytes per launch over its CUDA-event duration,
+  against the measured HBM copy bandwidth; ``roofline_sig_bulk`` the same for
+  the dense detection kernel.
 * ``plain``/``ragged``: the same implementation called once per frame
   (``remove_cosmics_device``) versus one batched plan, on this stack and on
   the ragged 64-frame batch with per-frame scalars.
@@ -48,6 +50,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Mpix/s (f64, maxiter=4, identical masks) batched vs plain; bwd/fwd time"
 SETTINGS = dict(contrast=3.0, cr_threshold=5.0, neighbor_threshold=3.0, maxiter=4)
 SIG_BULK_DRAM_BYTES_PER_PX = 8.62  # ncu: 144.6 MB per launch over 16.78 Mpix
+# ncu, prepare_bulk_kernel, one 16-frame stack launch (this workload):
+# 565.2 MB read + 514.2 MB written over 67.1 Mpix (written pixels still in
+# L2 at the end of the launch are not counted).
+PREPARE_DRAM_BYTES_PER_PX = 16.08
 
 
 def parse_args():
@@ -245,6 +251,33 @@ def main():
     kinds = _native.KERNEL_KINDS
     kms = {k: sum(p[0][k] for p in prof) / len(prof) for k in kinds}
     klaunch = {k: prof[0][1][k] for k in kinds}
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_source = "measured" if peaks else "fallback"
+    total_kernel_ms = sum(kms.values())
+
+    # The dominant kernel: prepare (holes, exclusions, clean pixels and the
+    # static bit planes, once per call), HBM-bound.  Per pixel it reads the
+    # float64 input (8 B) and the mask byte (1 B), writes clean (8 B) and the
+    # HOLE, EXCL and DONOR bit words (3/8 B).  This batch's frames (widths a
+    # multiple of 16, aligned buffers, no background map) take the bulk-staged
+    # variant.
+    prep_px = nf * h * w * klaunch["prepare"]
+    prep_bytes = prep_px * (8 + 1 + 8 + 3 / 8)
+    prep_ms = kms["prepare"]
+    prep_achieved = prep_bytes / (prep_ms / 1e3) / 1e9
+    prep_launch_px = prep_px / max(1, klaunch["prepare"])
+    roofline = {"bound": "hbm", "kernel": "prepare_bulk_kernel",
+                "achieved": round(prep_achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(prep_achieved / peak, 4),
+                "traffic": round(prep_launch_px * PREPARE_DRAM_BYTES_PER_PX),
+                "peak_source": peak_source,
+                "algorithmic_bytes_per_launch": round(prep_bytes / max(1, klaunch["prepare"])),
+                "avg_launch_ms": round(prep_ms / max(1, klaunch["prepare"]), 4),
+                "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
+                "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
+
     # Dense detection kernel (sig_bulk_kernel), run by the first (full) pass
     # over every frame.  Per pixel it reads clean (8 B); its bit planes were
     # zeroed by the call's prologue memset, and its writes (the sparse pre
@@ -255,21 +288,15 @@ def main():
     detect_bytes = active_px * 8
     detect_ms = kms["sigraw"]
     achieved = detect_bytes / (detect_ms / 1e3) / 1e9
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
-        if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
-    total_kernel_ms = sum(kms.values())
     # DRAM bytes per active pixel of one sig_bulk_kernel launch from an ncu
     # capture (profiles/sig_bulk_kernel_stack_2048_4frames.md), scaled to this
     # launch's active pixels.
     traffic = active_px * SIG_BULK_DRAM_BYTES_PER_PX / max(1, klaunch["sigraw"])
-    roofline = {"bound": "hbm", "kernel": "sig_bulk_kernel", "achieved": round(achieved, 1),
-                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": round(traffic), "peak_source": "measured" if peaks else "fallback",
-                "algorithmic_bytes_per_launch": round(detect_bytes / max(1, klaunch["sigraw"])),
-                "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4),
-                "kernel_ms": {k: round(v, 4) for k, v in kms.items() if v},
-                "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
+    roofline_sig_bulk = {"bound": "hbm", "kernel": "sig_bulk_kernel", "achieved": round(achieved, 1),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": round(traffic), "peak_source": peak_source,
+                         "algorithmic_bytes_per_launch": round(detect_bytes / max(1, klaunch["sigraw"])),
+                         "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4)}
     # Kernels of one execution as the event profiler saw them, plus those that
     # share a mark with another kernel: the replacement's target selection
     # (every pass) and the FRESH-plane zeroing that starts each incremental
@@ -283,7 +310,7 @@ def main():
            "config": dict(workload_config(args), parallelism=f"frames sharded, {world} GPU(s)",
                           path="plan + CUDA graph (while node)", passes=passes,
                           repeatable=identical),
-           "roofline": roofline, "clocks": clk, "gpu_launches": launches_per_step * args.steps}
+           "roofline": roofline, "roofline_sig_bulk": roofline_sig_bulk, "clocks": clk, "gpu_launches": launches_per_step * args.steps}
 
     # End to end through the host entry point, pinned host buffers.
     e2e_steps = max(2, min(args.steps, 5))

@@ -805,8 +805,8 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
 	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
 		(unsigned long long)L.total_px);
-	mark(rec, K_INIT);
 	if (!L.maxiter) {
+		mark(rec, K_INIT);
 		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
 		mark(rec, K_COPY);
 		return;
@@ -818,6 +818,7 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	check(cudaMemsetAsync(ws.bits.p + P_CRMASK * L.plane_words, 0,
 		(size_t)(N_PLANES - P_CRMASK) * L.plane_words * sizeof(uint32_t), s));
 	check(cudaMemsetAsync(ws.rowmarks.p, 0, 2 * (size_t)L.row_words * sizeof(uint32_t), s));
+	mark(rec, K_INIT); // the state and the zeroed planes
 	launch_prepare(ws, L, di, s);
 	mark(rec, K_PREPARE);
 	// Block floors: error-map thresholds; noise-model keys from prepare's row

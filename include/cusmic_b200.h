@@ -81,12 +81,12 @@ cusmic_plan_passes(cusmic_plan *plan, int *passes);
 /* Execute the plan once without its graph, with a CUDA event recorded on
  * stream after every kernel, then synchronise.  ms[k] and launches[k] receive
  * the summed duration and launch count of kernel kind k for k in 0..15:
- * init, prepare, hole fill, sig_raw (dense detection), candidates (5 x 5
- * medians), seeds (fine structure), grow/update, control, replace, restore,
- * zero-iteration copy, low candidates, classification of the dense pass's
- * list, block floors, and of the incremental passes the reclassification
- * with work-list gather and the dirty-row scan (kinds >= 16).  A timing aid; no counterpart in the
- * reference. */
+ * init (with the zeroing of the bit planes), prepare, hole fill, sig_raw
+ * (dense detection), candidates (5 x 5 medians), seeds (fine structure),
+ * grow/update, control, replace, restore, zero-iteration copy, low
+ * candidates, classification of the dense pass's list, block floors, and of
+ * the incremental passes the reclassification with work-list gather and the
+ * dirty-row scan.  A timing aid; no counterpart in the reference. */
 int
 cusmic_plan_profile(cusmic_plan *plan, void *stream, double *ms, int *launches, int kinds,
 	char *msg, size_t message_size);
