@@ -297,11 +297,10 @@ def main():
                          "traffic": round(traffic), "peak_source": peak_source,
                          "algorithmic_bytes_per_launch": round(detect_bytes / max(1, klaunch["sigraw"])),
                          "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4)}
-    # Kernels of one execution as the event profiler saw them, plus those that
-    # share a mark with another kernel: the replacement's target selection
-    # (every pass) and the FRESH-plane zeroing that starts each incremental
-    # pass.
-    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"] + 2 * klaunch["dirty"]
+    # Kernels of one execution as the event profiler saw them, plus the one
+    # that shares a mark with another kernel: the replacement's target
+    # selection (every pass).
+    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"] + klaunch["dirty"]
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),

@@ -699,17 +699,14 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	const int cap = di.sms * L.tune.dense_blocks_per_sm, sparse = di.sms * L.tune.sparse_blocks_per_sm;
 	const int rowb = L.tune.row_blocks_per_sm;
 	if (incremental) {
-		// FRESH of every frame (its growth visits a row list); the full pass
-		// finds S1, S2, CAND, FRESH and the growth row marks zeroed by the
-		// prologue.  In 16-byte words.
-		const long long n16 = L.plane_words / 4;
-		const long long blocks = (n16 + 255) / 256 < di.sms * 4 ? (n16 + 255) / 256 : di.sms * 4;
-		zero_words_kernel<<<(int)blocks, 256, 0, s>>>(
-			reinterpret_cast<uint4 *>(ws.bits.p + P_FRESH * L.plane_words), n16,
-			reinterpret_cast<uint4 *>(ws.rowmarks.p), 0);
-		const int tb = (nrows + 255) / 256 < di.sms * 4 ? (nrows + 255) / 256 : di.sms * 4;
+		// The dirty-row scan also zeroes FRESH of every frame (its growth
+		// visits a row list); the full pass finds S1, S2, CAND, FRESH and the
+		// growth row marks zeroed by the prologue.
+		const long long n16 = L.plane_words / 4; // 16-byte words of one plane
+		const long long need = ((n16 > nrows ? n16 : nrows) + 255) / 256;
+		const int tb = (int)(need < di.sms * 4 ? need : di.sms * 4);
 		dirty_rows_kernel<<<tb, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows, L.prm.mode,
-			ws.ctl.p, ws.dirty.p);
+			ws.ctl.p, ws.dirty.p, reinterpret_cast<uint4 *>(ws.bits.p + P_FRESH * L.plane_words), n16);
 		mark(rec, K_DIRTY);
 		const int rgrid = grid_for_rows(di, nrows, rowb);
 		if (L.error_frames)

@@ -109,13 +109,19 @@ __device__ __forceinline__ bool rows_changed(const FrameDesc &fd, int y, int r, 
 
 // The rows of active frames with a changed pixel within six rows, appended
 // to `out` (count in ctl->n_dirty) and marked for growth.  A thread per row.
+// The same threads first zero `clear` (n16 16-byte words: the FRESH plane,
+// which this pass's growth writes on the rows it visits and the previous
+// pass's replacement has read).
 __global__ void __launch_bounds__(256)
 dirty_rows_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
-	const int2 *__restrict__ rows, int nrows, int mode, Control *ctl, int2 *out)
+	const int2 *__restrict__ rows, int nrows, int mode, Control *ctl, int2 *out, uint4 *clear,
+	long long n16)
 {
 	const int lane = threadIdx.x & 31;
 	const bool wrap = mode == WRAP;
 	const int stride = gridDim.x * blockDim.x;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += stride)
+		clear[i] = make_uint4(0u, 0u, 0u, 0u);
 	for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nrows; base += stride) {
 		const int i = base + lane;
 		int2 item = make_int2(0, 0);

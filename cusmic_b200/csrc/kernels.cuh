@@ -88,17 +88,6 @@ validate_kernel(const double *__restrict__ v, long long n, int minimum, unsigned
 		atomicOr(flags, bit);
 }
 
-// Zero n 16-byte words at p and m at q (before a detection pass: the S1, S2,
-// CAND and FRESH planes of all frames, contiguous in the plane-major layout,
-// and the row marks).
-__global__ void __launch_bounds__(256) zero_words_kernel(uint4 *p, long long n, uint4 *q,
-	long long m)
-{
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n + m;
-	     i += (long long)gridDim.x * blockDim.x)
-		(i < n ? p[i] : q[i - n]) = make_uint4(0u, 0u, 0u, 0u);
-}
-
 __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
 	unsigned long long cand_cap)
 {
