@@ -591,3 +591,65 @@ def test_host_api_concurrent_calls(cuda):
         assert g is not None
         np.testing.assert_array_equal(g[1], wf)
         assert_bits_equal(g[0], wc)
+
+
+@pytest.mark.parametrize("mode", ("mirror", "constant"))
+@pytest.mark.parametrize("path", ("error", "model"))
+@pytest.mark.parametrize("shape", ((16, 16), (40, 48), (33, 80), (21, 528), (9, 1040)))
+def test_bulk_prepare_widths(cuda, oracle, mode, path, shape):
+    """Frames without a background map whose width is a multiple of 16 take the
+    bulk-staged prepare: half-filled last bit words (w % 32 == 16), a partial
+    last 512-pixel segment, holes, a mask and a scalar background; noise-model
+    frames also write their row minima there."""
+    h, w = shape
+    data, mask = small_scene(h * 31 + w, h, w, holes=0.01, masked=0.02, rays=max(1, h * w // 40))
+    frame = dict(data=data, mask=mask, background=25.0)
+    opts = dict(SETTINGS, border=mode, background=25.0)
+    if path == "error":
+        frame["error"] = np.sqrt(np.abs(np.nan_to_num(data)) + 9)
+    else:
+        frame.update(gain=1.5, readnoise=4.0)
+        opts.update(gain=1.5, readnoise=4.0)
+    check_against_oracle(oracle, [frame], opts)
+
+
+@pytest.mark.parametrize("mode", ("mirror", "wrap"))
+def test_bulk_prepare_ragged_mixed(cuda, oracle, mode):
+    """A ragged batch that takes the bulk-staged prepare (widths multiples of
+    16, no background maps) with error-map and noise-model frames mixed: row
+    minima only for the noise-model frames, per-frame scalar backgrounds."""
+    frames = []
+    for i, (h, w) in enumerate(((40, 48), (33, 528), (20, 16), (17, 1040), (64, 96))):
+        data, mask = small_scene(900 + i, h, w, holes=0.005, masked=0.01 if i % 2 else 0.0,
+                                 rays=max(2, h * w // 60))
+        f = dict(data=data, background=float(5 * i))
+        if mask is not None:
+            f["mask"] = mask
+        if i % 2 == 0:
+            f["error"] = np.sqrt(np.abs(np.nan_to_num(data)) / 1.5 + 16)
+        else:
+            f.update(gain=1.0 + 0.5 * i, readnoise=3.0 + i)
+        frames.append(f)
+    check_against_oracle(oracle, frames, dict(SETTINGS, border=mode), ragged=True)
+
+
+def test_prepare_unaligned_input(cuda, oracle):
+    """An input 8 bytes off a 16-byte boundary (float64-aligned, so accepted)
+    cannot be bulk-copied: that batch takes the register-staged prepare, with
+    the same bits."""
+    import torch
+    h, w = 40, 64
+    data, mask = small_scene(77, h, w, holes=0.01, masked=0.02, rays=30)
+    frame = dict(data=data, mask=mask, error=np.sqrt(np.abs(np.nan_to_num(data)) + 9))
+    fr = cabi.Frames([frame])
+    buf = torch.empty(h * w + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.from_numpy(data.ravel()).cuda()
+    fr.keep.append(buf)
+    fr.ims[0].data = buf.data_ptr() + 8
+    assert fr.ims[0].data % 16 == 8
+    st, msg = cabi.run_batch(cabi._native.lib(), fr, cabi.options(**SETTINGS))
+    assert st == 0, msg
+    want_clean, want_mask, _ = cabi.oracle_frame(oracle, frame, **SETTINGS)
+    (clean, got_mask), = fr.outputs()
+    np.testing.assert_array_equal(got_mask, want_mask)
+    assert_bits_equal(clean, want_clean)
