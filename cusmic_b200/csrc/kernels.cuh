@@ -251,9 +251,10 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 // One warp per row (grid-stride over the row list), in segments of 32 words
 // (1024 pixels): lane j keeps the HOLE, EXCL and DONOR words of the
 // segment's word j, so each plane gets one coalesced store per segment.  The
-// other planes were zeroed before the kernel.  Holes are not listed: the hole
-// fill scans the HOLE plane.
-// UL: the unroll of the kinds without maps.
+// other planes were zeroed before the kernel.  With `holes`, each segment's
+// holes are appended to that list (count in ctl->n_holes) for the hole fill.
+// KIND: the frame kind every row has (PREP_ANY: decided per row); UL: the
+// unroll of the kinds without maps.
 template <int KIND = PREP_ANY, int UL = ROW_UNROLL>
 __global__ void __launch_bounds__(256, 4)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
