@@ -50,7 +50,7 @@ def _worker(rank, world, port, sizes, out):
 
 def test_gather_metadata_two_ranks():
     sizes = [262144, 4194304, 65536, 1048576, 16384]
-    manager = mp.Manager()
+    manager = mp.get_context("spawn").Manager()  # no fork of this (threaded) process
     out = manager.dict()
     mp.spawn(_worker, args=(2, _free_port(), sizes, out), nprocs=2, join=True)
     want = [s % 97 for s in sizes]
