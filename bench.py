@@ -33,7 +33,6 @@ are independent, so no collective touches the data path.
 import argparse
 import ctypes
 import json
-import math
 import os
 import statistics
 import subprocess

@@ -7,7 +7,6 @@ bench.py may import this module; the product path never does.
 
 import ctypes
 import math
-from pathlib import Path
 
 import numpy as np
 

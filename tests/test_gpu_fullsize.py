@@ -9,7 +9,6 @@ oracle to run at that size:
 * the frozen-mask backward is linear in the incoming gradient.
 """
 
-import math
 
 import numpy as np
 import pytest
