@@ -11,9 +11,11 @@ pixels) are larger than the 126 MB L2, so no flush is needed between steps.
 * ``value``: Mpix/s with inputs resident in HBM, through a plan whose whole
   maxiter loop is one CUDA graph (device-side while node), timed with CUDA
   events on the launching stream, max over ranks.
-* ``e2e``: the same metric through the reference-facing host entry point
-  ``remove_cosmics`` (one call per frame, pinned host buffers in and out,
-  every copy inside the timed region).
+* ``e2e``: the same metric from host buffers to host buffers through the
+  C ABI's batch host entry point ``cusmic_batch_host`` (pinned buffers; every
+  copy inside the timed region; the shared maps cross PCIe once per step);
+  ``e2e_per_frame`` beside it: the reference-facing ``remove_cosmics``, one
+  call per frame, every map uploaded with every frame.
 * ``roofline``: the dominant kernel (prepare, the largest share of kernel
   time): its algorithmic bytes per launch over its CUDA-event duration,
   against the measured HBM copy bandwidth; ``roofline_sig_bulk`` the same for
@@ -21,9 +23,14 @@ pixels) are larger than the 126 MB L2, so no flush is needed between steps.
 * ``plain``/``ragged``: the same implementation called once per frame
   (``remove_cosmics_device``) versus one batched plan, on this stack and on
   the ragged 64-frame batch with per-frame scalars.
+* ``reference_gpu``: the reference's own CUDA library, compiled from its
+  sources for sm_100a, on the same resident inputs (a baseline leg, run after
+  this arm's timed region): its batch call on the stack, 64 per-frame calls on
+  the ragged batch, and whether its masks and pixels equal this library's on
+  every workload.
 * ``cpu_baseline``: the CPU oracle (a restatement of the reference's
-  algorithm; lacosmic 1.4.0 is not installed) on a bounded sample of the same
-  workload, all host threads.
+  algorithm; lacosmic 1.4.0 is not installed) on one full frame of the same
+  workload, all host threads, with a single-thread figure beside it.
 
 ``--impl reference`` times that CPU implementation alone as the reference arm.
 Multi-GPU (torchrun): every rank cleans its own stack (weak scaling); frames
@@ -38,6 +45,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -48,68 +56,124 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Mpix/s (f64, maxiter=4, identical masks) batched vs plain; bwd/fwd time"
 SETTINGS = dict(contrast=3.0, cr_threshold=5.0, neighbor_threshold=3.0, maxiter=4)
-SIG_BULK_DRAM_BYTES_PER_PX = 8.62  # ncu: 144.6 MB per launch over 16.78 Mpix
+# ncu, sig_bulk_kernel, 4-frame stack launch: 144.6 MB over 16.78 Mpix.
+SIG_BULK_DRAM_BYTES_PER_PX = 8.62
 # ncu, prepare_bulk_kernel, one 16-frame stack launch (this workload):
 # 565.2 MB read + 514.2 MB written over 67.1 Mpix (written pixels still in
 # L2 at the end of the launch are not counted).
 PREPARE_DRAM_BYTES_PER_PX = 16.08
+REF_GPU_SO = ROOT / "oracle" / "_ref" / "libcusmic_ref.so"
 
 
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=500)
-    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=5,
+                   help="warm-up executions at least (the warm-up also lasts at least "
+                        "--warm-seconds, so the clock sampler sees the GPU under load)")
+    p.add_argument("--warm-seconds", type=float, default=1.0)
     p.add_argument("--impl", choices=("mine", "reference"), default="mine")
     p.add_argument("--frames", type=int, default=16)
     p.add_argument("--size", type=int, default=2048)
-    p.add_argument("--no-extras", action="store_true", help="skip plain/ragged comparisons")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the plain/ragged/adjoint/large comparisons and the reference "
+                        "library leg")
     p.add_argument("--no-large", action="store_true", help="skip the 4 x 8192^2 forward/backward run")
-    p.add_argument("--cpu-sample-rows", type=int, default=1024,
-                   help="rows of one frame timed for the CPU baseline")
+    p.add_argument("--cpu-sample-rows", type=int, default=0,
+                   help="rows of one frame timed for the CPU baseline (0: the whole frame)")
     return p.parse_args()
 
 
 class Clocks:
-    """nvidia-smi samples (every 200 ms) taken while a region runs."""
+    """SM clock, power and throttle reasons sampled every few milliseconds by a
+    thread (NVML), or every 100 ms by nvidia-smi where NVML is not loadable;
+    mark() brackets the timed region so its own samples are reported."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, index):
+    def __init__(self, torch_device, period_s=0.002):
+        self.samples = []  # (time, sm MHz, max MHz, power W, reasons)
+        self.window = [None, None]
+        self.stop_flag = threading.Event()
+        self.proc = None
+        self.source = "nvml"
+        try:
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            props = torch.cuda.get_device_properties(torch_device)
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            self.nv, self.handle = nv, nv.nvmlDeviceGetHandleByPciBusId(bus)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.handle, nv.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._poll, args=(period_s,), daemon=True)
+            self.thread.start()
+        except Exception:
+            self.source = "nvidia-smi"
+            self._start_smi(torch_device)
+
+    def _poll(self, period_s):
+        nv, h = self.nv, self.handle
+        masks = [(name, getattr(nv, attr, 0)) for name, attr in self.REASONS]
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), sm, self.max_mhz, pw,
+                                     [n for n, m in masks if bits & m]))
+            except Exception:
+                pass
+            time.sleep(period_s)
+
+    def _start_smi(self, torch_device):
+        fields = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        index = os.environ.get("CUDA_VISIBLE_DEVICES", str(torch_device.index or 0)).split(",")[0]
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(index)], stdout=self.file, stderr=subprocess.DEVNULL)
+                ["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", index], stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
+    def mark(self, which):
+        self.window[which] = time.perf_counter()
+
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait()
-        self.file.seek(0)
-        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
-        os.unlink(self.file.name)
-        sm, mx, power, reasons = [], [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for r in rows:
-            try:
-                sm.append(float(r[1]))
-                mx.append(float(r[2]))
-                power.append(float(r[3]))
-            except (ValueError, IndexError):
-                continue
-            for name, v in zip(names, r[5:9]):
-                if v.strip().lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None,
-                "power_w_max": max(power) if power else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.source == "nvml":
+            self.stop_flag.set()
+            self.thread.join()
+        elif self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait()
+            self.file.seek(0)
+            for row in self.file.read().strip().splitlines():
+                r = [c.strip() for c in row.split(",")]
+                try:
+                    self.samples.append((None, float(r[0]), float(r[1]), float(r[2]),
+                                         [n for (n, _), v in zip(self.REASONS, r[3:7])
+                                          if v.lower().startswith("active")]))
+                except (ValueError, IndexError):
+                    continue
+            os.unlink(self.file.name)
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"],
+                    "samples": 0}
+        t0, t1 = self.window
+        timed = [s for s in self.samples if s[0] is not None and t0 <= s[0] <= t1]
+        under = timed or self.samples[-max(1, len(self.samples) // 2):]
+        reasons = sorted({r for s in under for r in s[4]})
+        return {"sm_mhz": statistics.median(s[1] for s in under) if under else None,
+                "sm_max_mhz": max(s[2] for s in under) if under else None,
+                "power_w_max": max(s[3] for s in under) if under else None,
+                "reasons": reasons, "samples": len(self.samples),
+                "samples_in_timed_region": len(timed), "source": self.source}
 
 
 def dist_setup(args):
@@ -120,9 +184,10 @@ def dist_setup(args):
 
 
 def cpu_reference(frame, error, mask, rows, threads=0):
-    """Time the CPU oracle on the first `rows` rows of one frame (all host
-    threads, or `threads` of them)."""
+    """Time the CPU oracle on the first `rows` rows of one frame (0: all rows),
+    with all host threads or `threads` of them."""
     from oracle import oracle
+    rows = rows or frame.shape[0]
     sub = np.ascontiguousarray(frame[:rows])
     prev = oracle.set_threads(0)
     oracle.set_threads(threads or os.cpu_count())
@@ -139,13 +204,15 @@ def cpu_reference(frame, error, mask, rows, threads=0):
 def cpu_single_thread(frame, error, mask, rows):
     """The CPU oracle on one host thread (a like-for-like stand-in for a
     single-threaded CPU implementation), on an eighth of the sample rows."""
+    rows = rows or frame.shape[0]
     v, dt, n = cpu_reference(frame, error, mask, max(32, rows // 8), threads=1)
     return {"value": round(v, 4), "unit": "Mpix/s", "cores": 1,
             "sample": f"{n // frame.shape[1]}x{frame.shape[1]} rows of frame 0 ({n} px, {dt:.1f} s)"}
 
 
 def run_reference_arm(args, world, rank):
-    """The reference's algorithm on the host cores (CPU oracle, all threads)."""
+    """The reference's algorithm on the host cores (CPU oracle, all threads),
+    one full frame of the stack per step."""
     if rank != 0:
         return
     from cusmic_b200 import scenes
@@ -161,8 +228,9 @@ def run_reference_arm(args, world, rank):
     dt = time.perf_counter() - t0
     value = px / dt / 1e6
     cores = os.cpu_count()
-    sample = (f"{args.cpu_sample_rows}x{args.size} rows of one {args.size}x{args.size} frame of "
-              f"the stack per step, maxiter=4, OpenMP over {cores} threads")
+    rows = args.cpu_sample_rows or args.size
+    sample = (f"{rows}x{args.size} rows of one {args.size}x{args.size} frame of the stack per "
+              f"step, maxiter=4, OpenMP over {cores} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mpix/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -218,22 +286,29 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    smi_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0]
-    clocks = Clocks(smi_index if smi_index.isdigit() else local)
-    for _ in range(args.warmup):
+    clocks = Clocks(dev)
+    # Warm-up: at least --warmup executions and --warm-seconds of GPU work, so
+    # the clocks have settled under load when the timed region starts.
+    warm, t_warm = 0, time.perf_counter()
+    while warm < args.warmup or time.perf_counter() - t_warm < args.warm_seconds:
         plan.execute(stream)
+        warm += 1
+        if warm % 64 == 0:
+            stream.synchronize()
     plan.wait()
     passes = plan.passes()
     ref_clean = batch.clean.clone()
     ref_mask = batch.mask_out.clone()
 
     barrier()
+    clocks.mark(0)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
     for _ in range(args.steps):
         plan.execute(stream)
     end.record(stream)
     barrier()
+    clocks.mark(1)
     clk = clocks.stop()
     plan.wait()
     ms = start.elapsed_time(end)
@@ -287,9 +362,8 @@ def main():
     detect_bytes = active_px * 8
     detect_ms = kms["sigraw"]
     achieved = detect_bytes / (detect_ms / 1e3) / 1e9
-    # DRAM bytes per active pixel of one sig_bulk_kernel launch from an ncu
-    # capture (profiles/sig_bulk_kernel_stack_2048_4frames.md), scaled to this
-    # launch's active pixels.
+    # DRAM bytes per active pixel of one launch from an ncu capture of the
+    # 4-frame stack, scaled to this launch's active pixels.
     traffic = active_px * SIG_BULK_DRAM_BYTES_PER_PX / max(1, klaunch["sigraw"])
     roofline_sig_bulk = {"bound": "hbm", "kernel": "sig_bulk_kernel", "achieved": round(achieved, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -307,58 +381,29 @@ def main():
            "data": "synthetic (seeded scene generator, inputs resident in HBM)",
            "config": dict(workload_config(args), parallelism=f"frames sharded, {world} GPU(s)",
                           path="plan + CUDA graph (while node)", passes=passes,
-                          repeatable=identical),
-           "roofline": roofline, "roofline_sig_bulk": roofline_sig_bulk, "clocks": clk, "gpu_launches": launches_per_step * args.steps}
+                          repeatable=identical, warmup_executions=warm),
+           "roofline": roofline, "roofline_sig_bulk": roofline_sig_bulk, "clocks": clk,
+           "gpu_launches": launches_per_step * args.steps}
 
-    # End to end through the host entry point, pinned host buffers.
-    e2e_steps = max(2, min(args.steps, 5))
-    L = _native.lib()
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    h_data = [pin(f.data) for f in sc.frames]
-    h_err, h_mask = pin(sc.error), pin(sc.mask.astype(np.uint8))
-    h_clean = torch.empty((h, w), dtype=torch.float64).pin_memory()
-    h_flags = torch.empty((h, w), dtype=torch.uint8).pin_memory()
-    o = plan.options
-    msg = ctypes.create_string_buffer(256)
-
-    def host_step():
-        for f in range(nf):
-            im = _native.Image(h_data[f].data_ptr(), h_err.data_ptr(), None, None, None,
-                               h_mask.data_ptr(), w, h)
-            st = L.remove_cosmics(ctypes.byref(im), ctypes.byref(o), h_clean.data_ptr(),
-                                  h_flags.data_ptr(), msg, 256)
-            if st:
-                raise RuntimeError(msg.value.decode())
-    host_step()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        host_step()
-    barrier()
-    e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_s = float(e2e_t.item())
-    out["e2e"] = {"value": round(world * total_px * e2e_steps / e2e_s / 1e6, 2), "unit": "Mpix/s",
-                  "h2d_bytes_per_step": nf * h * w * (8 + 8 + 1),
-                  "d2h_bytes_per_step": nf * h * w * (8 + 1),
-                  "path": "remove_cosmics (host C ABI), one call per frame, pinned buffers"}
-    last_frame_ok = bool(np.array_equal(h_flags.numpy(), batch.mask_out[-1].cpu().numpy()))
-    out["e2e"]["identical_masks"] = last_frame_ok
+    out["e2e"], out["e2e_per_frame"] = end_to_end(sc, plan, batch, args, world, barrier)
 
     if not args.no_extras and world == 1:  # single-GPU comparisons
         out["plain"] = plain_vs_batched(plan, batch, stream, value / world, barrier)
-        out["ragged"] = ragged_comparison(dev, stream, barrier)
-        out["adjoint"] = adjoint_timing(dev, stream, barrier)
+        ragged, ragged_ctx = ragged_comparison(dev, stream, barrier)
+        out["ragged"] = ragged
+        out["adjoint"], adjoint_ctx = adjoint_timing(dev, stream, barrier)
+        out["reference_gpu"] = reference_gpu(plan, batch, ragged_ctx, adjoint_ctx, value,
+                                             ragged["batched_mpix_s"], stream, dev)
         if not args.no_large:
-            out["large"] = large_run(dev, stream, barrier)
+            out["large"] = large_run(dev, stream, barrier, out["reference_gpu"])
+        ragged_ctx["plan"].close()
+        adjoint_ctx["plan"].close()
 
     if rank == 0:
         v, dt, n = cpu_reference(sc.frames[0].data, sc.error, sc.mask, args.cpu_sample_rows)
         out["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpix/s", "cores": os.cpu_count(),
                                "kind": "port",
-                               "sample": f"{args.cpu_sample_rows}x{w} rows of frame 0 "
+                               "sample": f"{n // w}x{w} rows of frame 0 "
                                          f"({n} px, {dt:.1f} s), maxiter=4, OpenMP threads",
                                "single_thread": cpu_single_thread(
                                    sc.frames[0].data, sc.error, sc.mask, args.cpu_sample_rows)}
@@ -368,9 +413,79 @@ def main():
         dist.destroy_process_group()
 
 
+def end_to_end(sc, plan, batch, args, world, barrier):
+    """Host buffers in, host buffers out, every copy inside the timed region:
+    the batch host entry point (the headline), and the reference-facing
+    single-frame host call once per frame beside it."""
+    import torch
+    from cusmic_b200 import _native
+    nf, h, w = args.frames, args.size, args.size
+    total_px = nf * h * w
+    dev = batch.clean.device
+    L = _native.lib()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    h_stack = pin(np.stack([f.data for f in sc.frames]))
+    h_err, h_mask = pin(sc.error), pin(sc.mask.astype(np.uint8))
+    h_clean = torch.empty((nf, h, w), dtype=torch.float64).pin_memory()
+    h_flags = torch.empty((nf, h, w), dtype=torch.uint8).pin_memory()
+    o = plan.options
+    msg = ctypes.create_string_buffer(256)
+    ims = (_native.Image * nf)()
+    for f in range(nf):
+        ims[f] = _native.Image(h_stack[f].data_ptr(), h_err.data_ptr(), None, None, None,
+                               h_mask.data_ptr(), w, h)
+
+    def batch_step():
+        st = L.cusmic_batch_host(ims, nf, ctypes.byref(o), None, h_clean.data_ptr(),
+                                 h_flags.data_ptr(), msg, 256)
+        if st:
+            raise RuntimeError(msg.value.decode())
+
+    def frame_step():
+        for f in range(nf):
+            st = L.remove_cosmics(ctypes.byref(ims[f]), ctypes.byref(o),
+                                  h_clean[f].data_ptr(), h_flags[f].data_ptr(), msg, 256)
+            if st:
+                raise RuntimeError(msg.value.decode())
+
+    def timed(step, reps):
+        step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            step()
+        barrier()
+        t = torch.tensor([time.perf_counter() - t0], device=dev, dtype=torch.float64)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return world * total_px * reps / float(t.item()) / 1e6
+
+    reps = max(3, min(args.steps, 10))
+    v_batch = timed(batch_step, reps)
+    same_batch = bool(torch.equal(h_flags.to(dev), batch.mask_out)) and bool(
+        torch.equal(h_clean.to(dev).view(torch.int64), batch.clean.view(torch.int64)))
+    v_frame = timed(frame_step, max(2, min(args.steps, 5)))
+    same_frame = bool(torch.equal(h_flags.to(dev), batch.mask_out)) and bool(
+        torch.equal(h_clean.to(dev).view(torch.int64), batch.clean.view(torch.int64)))
+    e2e = {"value": round(v_batch, 2), "unit": "Mpix/s",
+           "h2d_bytes_per_step": total_px * 8 + h * w * (8 + 1),
+           "d2h_bytes_per_step": total_px * (8 + 1),
+           "path": "cusmic_batch_host (host C ABI, whole stack per call: chunks of frames, "
+                   "inbound copy, cleaning and outbound copy of neighbouring chunks "
+                   "overlapped; shared error map and mask uploaded once), pinned buffers",
+           "identical_to_resident": same_batch}
+    per_frame = {"value": round(v_frame, 2), "unit": "Mpix/s",
+                 "h2d_bytes_per_step": total_px * (8 + 8 + 1),
+                 "d2h_bytes_per_step": total_px * (8 + 1),
+                 "path": "remove_cosmics (host C ABI, the reference's single-frame call), one "
+                         "call per frame, pinned buffers",
+                 "identical_to_resident": same_frame}
+    return e2e, per_frame
+
+
 def plain_vs_batched(plan, batch, stream, batched_value, barrier):
     """Per-frame remove_cosmics_device calls of the same implementation."""
-    import torch
     from cusmic_b200 import _native
     L = _native.lib()
     o = plan.options
@@ -449,10 +564,10 @@ def ragged_comparison(dev, stream, barrier):
         step()
     barrier()
     plain = px * 3 / (time.perf_counter() - t0) / 1e6
-    plan.close()
-    return {"frames": len(frames), "pixels": px, "batched_mpix_s": round(batched, 2),
-            "plain_mpix_s": round(plain, 2), "batched_over_plain": round(batched / plain, 3),
-            "identical_masks": bool(same), "kernel_ms": kernel_ms}
+    return ({"frames": len(frames), "pixels": px, "batched_mpix_s": round(batched, 2),
+             "plain_mpix_s": round(plain, 2), "batched_over_plain": round(batched / plain, 3),
+             "identical_masks_plain_vs_batched": bool(same), "kernel_ms": kernel_ms},
+            {"plan": plan, "batch": batch, "frames": frames})
 
 
 # Cycles of the sleep kernel ahead of a gated interval (about 0.27 ms at
@@ -479,9 +594,101 @@ def gated_ms(stream, call):
     return s.elapsed_time(e), out
 
 
-def large_run(dev, stream, barrier):
+def reference_lib():
+    """The reference's CUDA library built from its own sources (oracle/build.py)
+    for the baseline leg, or None when it was not built."""
+    if not REF_GPU_SO.exists():
+        return None
+    from cusmic_b200 import _native
+    L = ctypes.CDLL(str(REF_GPU_SO))
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    L.remove_cosmics_batch_device.restype = ctypes.c_int
+    L.remove_cosmics_batch_device.argtypes = [ctypes.POINTER(_native.Image), sz,
+                                              ctypes.POINTER(_native.Options), vp, vp, vp,
+                                              ctypes.c_char_p, sz]
+    return L
+
+
+def same_outputs(torch, a_clean, a_mask, b_clean, b_mask):
+    return bool(torch.equal(a_mask, b_mask)) and bool(
+        torch.equal(a_clean.view(torch.int64), b_clean.view(torch.int64)))
+
+
+def reference_gpu(plan, batch, ragged, adjoint, value, ragged_value, stream, dev):
+    """Baseline leg: the reference's own CUDA library on the same resident
+    inputs, after this arm's timed region.  Its device calls allocate their
+    scratch and synchronise per pass, as its stock path does; each call is
+    timed with CUDA events on the stream it runs on.  Also records whether
+    its outputs equal this library's bit for bit."""
+    import torch
+    L = reference_lib()
+    if L is None:
+        return {"unavailable": "oracle/_ref/libcusmic_ref.so was not built"}
+    msg = ctypes.create_string_buffer(512)
+    out = {"library": "reference src/api.cu compiled for sm_100a (--fmad=false, -O2)"}
+
+    def call(ims, nf, opts, clean, mask):
+        st = L.remove_cosmics_batch_device(ims, nf, ctypes.byref(opts), clean, mask,
+                                           stream.cuda_stream, msg, 512)
+        if st:
+            raise RuntimeError("reference library: " + msg.value.decode())
+
+    def events(fn, reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e) / reps, (time.perf_counter() - t0) * 1e3 / reps
+
+    # stack_2048: one batch call per step.
+    nf = len(batch.frames)
+    ims = batch.images()
+    r_clean, r_mask = torch.empty_like(batch.clean), torch.empty_like(batch.mask_out)
+    ms, wall = events(lambda: call(ims, nf, plan.options, r_clean.data_ptr(), r_mask.data_ptr()),
+                      3)
+    px = batch.total
+    out["stack_2048"] = {"mpix_s": round(px / (ms / 1e3) / 1e6, 2), "ms_per_step": round(ms, 3),
+                         "wall_ms_per_step": round(wall, 3),
+                         "mine_over_reference": round(value / (px / (ms / 1e3) / 1e6), 2),
+                         "identical": same_outputs(torch, r_clean, r_mask, batch.clean,
+                                                   batch.mask_out)}
+    # ragged_64: its scalars are batch-wide, so one call per frame.
+    rb, rp = ragged["batch"], ragged["plan"]
+    rims = rb.images()
+    rc, rm = torch.empty_like(rb.clean), torch.empty_like(rb.mask_out)
+    opts = [rp.options_for(i) for i in range(len(rb.frames))]
+
+    def per_frame():
+        for i in range(len(rb.frames)):
+            call(ctypes.byref(rims[i]), 1, opts[i], rc.data_ptr() + 8 * rb.offsets[i],
+                 rm.data_ptr() + rb.offsets[i])
+    ms, wall = events(per_frame, 2)
+    rp.execute(stream)
+    rp.wait()
+    out["ragged_64"] = {"mpix_s": round(rb.total / (ms / 1e3) / 1e6, 2),
+                        "ms_per_step": round(ms, 3), "wall_ms_per_step": round(wall, 3),
+                        "calls_per_step": len(rb.frames),
+                        "mine_over_reference": round(ragged_value / (rb.total / (ms / 1e3) / 1e6), 2),
+                        "identical": same_outputs(torch, rc, rm, rb.clean, rb.mask_out)}
+    # adjoint_1024 forward: identity of the outputs only.
+    ab, ap = adjoint["batch"], adjoint["plan"]
+    ap.execute(stream)
+    ap.wait()
+    ac, am = torch.empty_like(ab.clean), torch.empty_like(ab.mask_out)
+    call(ab.images(), len(ab.frames), ap.options, ac.data_ptr(), am.data_ptr())
+    out["adjoint_1024"] = {"identical": same_outputs(torch, ac, am, ab.clean, ab.mask_out)}
+    return out
+
+
+def large_run(dev, stream, barrier, reference_out=None):
     """large_8192: forward and frozen-mask backward of 4 x 8192^2 float64 frames
-    (full-size error map, 2% mask), with the device memory the process holds."""
+    (full-size error map, 2% mask), with the device memory the process holds;
+    the reference library's forward on the same inputs is compared once."""
     import torch
     from cusmic_b200 import scenes
     from cusmic_b200.plan import Plan, Batch
@@ -519,6 +726,21 @@ def large_run(dev, stream, barrier):
            "repeatable": bool(torch.equal(first_mask, batch.mask_out)),
            "device_gb_held": round((total - free1) / 1e9, 2),
            "device_gb_before": round((total - free0) / 1e9, 2)}
+    L = reference_lib()
+    if reference_out is not None and L is not None:
+        msg = ctypes.create_string_buffer(512)
+        rc, rm = torch.empty_like(batch.clean), torch.empty_like(batch.mask_out)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        st = L.remove_cosmics_batch_device(batch.images(), len(batch.frames),
+                                           ctypes.byref(plan.options), rc.data_ptr(),
+                                           rm.data_ptr(), stream.cuda_stream, msg, 512)
+        ms = (time.perf_counter() - t0) * 1e3
+        reference_out["large_8192"] = (
+            {"error": msg.value.decode()} if st else
+            {"wall_ms": round(ms, 1), "mpix_s": round(px / (ms / 1e3) / 1e6, 1),
+             "identical": same_outputs(torch, rc, rm, batch.clean, batch.mask_out)})
+        del rc, rm
     plan.close()
     del batch, stack, g
     torch.cuda.empty_cache()
@@ -551,10 +773,10 @@ def adjoint_timing(dev, stream, barrier):
         fwd += t
         t, _ = gated_ms(side, lambda: plan.backward(g, side))
         bwd += t
-    plan.close()
-    return {"workload": "adjoint_1024: 8 x 1024x1024, gain=2 rn=5 bg=0, L = sum(w * cleaned)",
-            "fwd_ms": round(fwd / reps, 4), "bwd_ms": round(bwd / reps, 4),
-            "bwd_over_fwd": round(bwd / fwd, 4)}
+    return ({"workload": "adjoint_1024: 8 x 1024x1024, gain=2 rn=5 bg=0, L = sum(w * cleaned)",
+             "fwd_ms": round(fwd / reps, 4), "bwd_ms": round(bwd / reps, 4),
+             "bwd_over_fwd": round(bwd / fwd, 4)},
+            {"plan": plan, "batch": batch})
 
 
 if __name__ == "__main__":

@@ -14,6 +14,7 @@ LIB_PATH = Path(__file__).with_name("libcusmic_b200.so")
 CUSMIC_OK, CUSMIC_INVALID, CUSMIC_CUDA_ERROR, CUSMIC_NO_MEMORY = range(4)
 BORDERS = {"reflect": 0, "constant": 1, "nearest": 2, "mirror": 3, "wrap": 4}
 PLAN_GRAPH, PLAN_KEEP = 1, 2
+FAULT_PREPARE_WAIT, FAULT_DETECT_WAIT, FAULT_NO_MEMORY = 1, 2, 3
 
 # Every symbol declared in include/cusmic.h and include/cusmic_b200.h.
 EXPORTS = (
@@ -22,6 +23,7 @@ EXPORTS = (
     "cusmic_plan_create", "cusmic_plan_bind", "cusmic_plan_execute", "cusmic_plan_wait",
     "cusmic_plan_passes", "cusmic_plan_profile", "cusmic_plan_backward", "cusmic_plan_destroy",
     "remove_cosmics_device_noalloc", "cusmic_set_tuning", "cusmic_get_tuning",
+    "cusmic_inject_fault", "cusmic_batch_host",
 )
 TUNING_PATH = Path(__file__).with_name("tuning.json")
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
@@ -116,6 +118,10 @@ def lib():
     L.cusmic_set_tuning.argtypes = [ctypes.POINTER(Tuning), sz, cp, sz]
     L.cusmic_get_tuning.restype = ip
     L.cusmic_get_tuning.argtypes = [sz, ctypes.POINTER(Tuning)]
+    L.cusmic_batch_host.restype = ip
+    L.cusmic_batch_host.argtypes = [img, sz, opt, sca, vp, vp, cp, sz]
+    L.cusmic_inject_fault.restype = ip
+    L.cusmic_inject_fault.argtypes = [ip, ctypes.c_longlong]
     _lib = L
     if TUNING_PATH.exists():
         set_tuning(json.loads(TUNING_PATH.read_text())["table"])

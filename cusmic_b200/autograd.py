@@ -8,11 +8,63 @@ other pixel, and the background add/subtract, pass it straight through.
 """
 
 import math
+import threading
 
 import torch
 
 from .api import Cleaner, Image
 from .plan import Batch, Plan
+
+# Idle plans per batch signature (device, shapes, which maps are present and
+# how they are shared, options).  A forward takes one (or creates it) and binds
+# it to its tensors; the plan goes back when the autograd graph that holds it
+# is freed, so a graph kept for a second backward keeps its frozen mask.
+_IDLE = {}
+_IDLE_PER_KEY = 2
+_LOCK = threading.Lock()
+
+
+class _Lease:
+    """A plan held by one autograd graph; returned to the idle pool when the
+    graph (and with it this object) is freed."""
+
+    def __init__(self, key, plan):
+        self.key, self.plan = key, plan
+
+    def __del__(self):
+        try:
+            with _LOCK:
+                idle = _IDLE.setdefault(self.key, [])
+                if len(idle) < _IDLE_PER_KEY:
+                    idle.append(self.plan)
+                    return
+            self.plan.close()
+        except Exception:
+            pass
+
+
+def _signature(batch, options):
+    def kind(maps):
+        present = [m is not None for m in maps]
+        shared = len({m.data_ptr() for m in maps if m is not None}) <= 1
+        return (tuple(present), shared)
+    # NaN (no value) compares unequal to itself: key it as None.
+    opts = tuple(sorted((k, None if isinstance(v, float) and math.isnan(v) else v)
+                        for k, v in options.items()))
+    return (batch.device, tuple(batch.sizes), kind(batch.errors), kind(batch.masks),
+            kind(batch.gains), kind(batch.readnoises), kind(batch.backgrounds), opts)
+
+
+def _plan_for(batch, options):
+    key = _signature(batch, options)
+    with _LOCK:
+        idle = _IDLE.get(key)
+        plan = idle.pop() if idle else None
+    if plan is None:
+        plan = Plan(batch, graph=True, keep=True, **options)
+    else:
+        plan.bind(batch)
+    return _Lease(key, plan)
 
 
 class _Clean(torch.autograd.Function):
@@ -30,15 +82,18 @@ class _Clean(torch.autograd.Function):
                             background=bg if _is_map(bg) else None)
         gain = float(image.effective_gain) if _is_scalar(image.effective_gain) else math.nan
         rn = float(image.readnoise) if _is_scalar(image.readnoise) else 0.0
-        plan = Plan(batch, graph=False, keep=True, contrast=float(cleaner.contrast),
-                    cr_threshold=float(cleaner.cr_threshold),
-                    neighbor_threshold=float(cleaner.neighbor_threshold),
-                    maxiter=int(cleaner.maxiter), border=cleaner.border_mode,
-                    gain=gain if image.error is None else math.nan,
-                    readnoise=rn if image.error is None else 0.0,
-                    background=float(bg) if scalar_bg else math.nan)
+        options = dict(contrast=float(cleaner.contrast),
+                       cr_threshold=float(cleaner.cr_threshold),
+                       neighbor_threshold=float(cleaner.neighbor_threshold),
+                       maxiter=int(cleaner.maxiter), border=cleaner.border_mode,
+                       gain=gain if image.error is None else math.nan,
+                       readnoise=rn if image.error is None else 0.0,
+                       background=float(bg) if scalar_bg else math.nan)
+        lease = _plan_for(batch, options)
+        plan = lease.plan
         plan.execute()
         plan.wait()
+        ctx.lease = lease
         ctx.plan = plan
         ctx.shape = data.shape
         ctx.bg_shape = None if bg is None else tuple(bg.shape)

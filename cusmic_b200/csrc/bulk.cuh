@@ -106,6 +106,7 @@ struct __align__(128) BulkRing {
 	int2 meta[BK_SLOTS];           // first ring row of an item: {item index, y1}; index < 0: end
 	int shift[BK_SLOTS];           // 0 or 1
 	unsigned long long full[BK_SLOTS], empty[BK_SLOTS];
+	unsigned long long poison; // never completes (injected failures only)
 	int abort;
 };
 
@@ -164,8 +165,9 @@ __device__ __forceinline__ bool mbar_test(unsigned long long *b, unsigned parity
 }
 
 // Wait until the phase of parity `parity` of barrier b has completed; false
-// after about BK_WAIT_CYCLES SM cycles, or as soon as the block aborted.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, const int *abort)
+// after about `limit` SM cycles, or as soon as the block aborted.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, const int *abort,
+	long long limit = BK_WAIT_CYCLES)
 {
 	if (mbar_test(b, parity))
 		return true;
@@ -173,9 +175,17 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
 	for (unsigned i = 1;; ++i) {
 		if (mbar_test(b, parity))
 			return true;
-		if ((i & 15) == 0 && (*(const volatile int *)abort || clock64() - t0 > BK_WAIT_CYCLES))
+		if ((i & 15) == 0 && (*(const volatile int *)abort || clock64() - t0 > limit))
 			return false;
 	}
+}
+
+// An injected failure (Control::poison_wait): a wait, bounded by `limit`
+// cycles, on barrier b, which was initialised for one arrival that never
+// comes.  It runs out and returns false, like a wait whose copies never land.
+__device__ __forceinline__ bool poisoned_wait(unsigned long long *b, const int *abort, long long limit)
+{
+	return mbar_wait(b, 0, abort, limit);
 }
 
 // Global -> shared bulk copy completing on barrier bar (16-byte aligned
@@ -667,6 +677,7 @@ sig_bulk_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 			mbar_init(&R.full[i], 2); // producer lanes 0 (bytes) and 1 (cp.async)
 			mbar_init(&R.empty[i], BK_CWARPS);
 		}
+		mbar_init(&R.poison, 1);
 		R.abort = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 	}
@@ -675,6 +686,8 @@ sig_bulk_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 	int issued = 0; // ring rows issued (producer warp)
 	if (warp == BK_CWARPS)
 		ok = bulk_producer(R, frames, state, items, nitems, lap_mode(prm.mode), ctl, issued);
+	else if (warp == 0 && blockIdx.x == 0 && ctl->poison_wait[1] > 0)
+		ok = __all_sync(0xffffffffu, poisoned_wait(&R.poison, &R.abort, ctl->poison_wait[1]));
 	else
 		ok = bulk_consumer(R, frames, items, prm, pre, pre_counts);
 	if (!ok && lane == 0) {
@@ -770,6 +783,11 @@ classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 	__shared__ ClassifyStage H, L;
 	__shared__ unsigned long long bases[2];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	// After a bounded wait of the dense kernel ran out, the counts of the
+	// items it left are stale: list nothing (the loop control then stops
+	// every frame and the call reports the fault).
+	if (*(const volatile int *)&ctl->fault)
+		return;
 	if (threadIdx.x == 0) {
 		H.n = L.n = 0;
 		H.fail = L.fail = CL_CAP;

@@ -138,6 +138,10 @@ struct Control {
 	int n_dirty;                  // this pass: length of the dirty-row list
 	unsigned n_sel;               // this pass: targets the replacement visits
 	unsigned pad;
+	// Injected failures (0: none): the bound, in SM cycles, of one extra wait
+	// on a barrier that nothing completes, made by one warp of the first block
+	// of the bulk-staged prepare ([0]) and of the dense detection kernel ([1]).
+	long long poison_wait[2];
 };
 
 CB_HD uint32_t *plane_ptr(const FrameDesc &f, int p)

@@ -18,6 +18,7 @@
 #include "backward.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <condition_variable>
@@ -51,6 +52,21 @@ static void check(cudaError_t e)
 		throw std::runtime_error(cudaGetErrorString(e));
 }
 
+// Injected failures (cusmic_inject_fault): the bounds of the injected device
+// waits of calls that start later, and the number of workspace reservations
+// still to fail as an exhausted allocator would.
+static std::atomic<long long> inject_wait[2] = {{0}, {0}};
+static std::atomic<long long> inject_alloc_failures{0};
+
+// True when this reservation is one that an injection makes fail.
+static bool injected_alloc_failure()
+{
+	long long left = inject_alloc_failures.load();
+	while (left > 0)
+		if (inject_alloc_failures.compare_exchange_weak(left, left - 1))
+			return true;
+	return false;
+}
 
 template <class T> struct DevBuf {
 	T *p = nullptr;
@@ -60,13 +76,14 @@ template <class T> struct DevBuf {
 	DevBuf &operator=(const DevBuf &) = delete;
 	void ensure(size_t want)
 	{
-		if (want <= n)
+		const bool fail = injected_alloc_failure();
+		if (want <= n && !fail)
 			return;
 		if (p)
 			cudaFree(p);
 		p = nullptr;
 		n = 0;
-		if (want > SIZE_MAX / sizeof(T))
+		if (want > SIZE_MAX / sizeof(T) || fail)
 			throw std::bad_alloc();
 		check(cudaMalloc(&p, want * sizeof(T)));
 		n = want;
@@ -86,12 +103,15 @@ template <class T> struct PinBuf {
 	PinBuf &operator=(const PinBuf &) = delete;
 	void ensure(size_t want)
 	{
-		if (want <= n)
+		const bool fail = injected_alloc_failure();
+		if (want <= n && !fail)
 			return;
 		if (p)
 			cudaFreeHost(p);
 		p = nullptr;
 		n = 0;
+		if (fail)
+			throw std::bad_alloc();
 		check(cudaMallocHost(&p, want * sizeof(T)));
 		n = want;
 	}
@@ -320,6 +340,7 @@ struct Layout {
 	int maxiter = 0;
 	int error_frames = 0; // frames with an error map (a rebound plan keeps which)
 	cusmic_tuning tune{};
+	long long poison_wait[2] = {0, 0}; // injected failures in force when the batch was laid out
 };
 
 struct DeviceInfo {
@@ -371,6 +392,11 @@ struct Workspace {
 	DevBuf<uint8_t> hmask, hout;
 	HostStage stage_io; // pageable host buffers of the host entry point
 	DevBuf<unsigned> hflags; // failed map checks of the host entry point
+	// Host-buffer batch (cusmic_batch_host): maps shared by several frames,
+	// and the pinned copies of a chunk's state and map-check flags.
+	DevBuf<double> hshared;
+	DevBuf<uint8_t> hshared_mask;
+	PinBuf<unsigned> hflags_host;
 };
 
 static std::mutex pool_mu;
@@ -502,6 +528,8 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		: item_rows(ims, nf, di.sms * tune.dense_blocks_per_sm);
 	Layout L;
 	L.tune = tune;
+	L.poison_wait[0] = inject_wait[0].load();
+	L.poison_wait[1] = inject_wait[1].load();
 	L.maxiter = o.maxiter;
 	L.prm.contrast = o.contrast;
 	L.prm.cr = o.cr_threshold;
@@ -801,7 +829,7 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
 	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
-		(unsigned long long)L.total_px);
+		(unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1]);
 	if (!L.maxiter) {
 		mark(rec, K_INIT);
 		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
@@ -1045,6 +1073,316 @@ extern "C" int cusmic_ragged_batch_device(const cusmic_image *ims, size_t nf,
 	return guarded([&] {
 		check_arguments(ims, nf, o, sc, clean, mask, false);
 		run_device(ims, nf, *o, sc, clean, mask, (cudaStream_t)stream);
+	}, msg, len);
+}
+
+// ---------------------------------------------------------------------------
+// Host-buffer batch.  The reference's host entry point cleans one frame and
+// moves its maps and pixels with blocking copies (src/api.cu:116-153); a
+// batch of frames called that way pays every map again per frame and never
+// overlaps a frame's inbound copy with the previous frame's outbound copy.
+// Here frames are cleaned in chunks of whole frames on three streams: chunk
+// k + 1's pixels go up while chunk k is cleaned and chunk k - 1's results
+// come down (PCIe moves both directions at once), and a map that several
+// frames share is uploaded and checked once per call.
+
+namespace cb {
+
+constexpr size_t HB_CHUNK_BYTES = size_t(24) << 20; // input bytes a chunk aims for
+constexpr size_t HB_ALIGN = 16;                     // pixels: chunk offsets stay 16-byte aligned
+
+static size_t hb_round(size_t n)
+{
+	return (n + HB_ALIGN - 1) / HB_ALIGN * HB_ALIGN;
+}
+
+// The map-check flags of validate_kernel, in the reference's order of checks
+// (src/api.cu:161-168).
+static void throw_map_flags(unsigned bad)
+{
+	if (bad & 1u)
+		throw InvalidArgument("error must be finite and positive");
+	if (bad & 2u)
+		throw InvalidArgument("gain must be finite and positive");
+	if (bad & 4u)
+		throw InvalidArgument("read noise must be finite and nonnegative");
+	if (bad & 8u)
+		throw InvalidArgument("background must be finite");
+}
+
+// Streams and events of one call; on every exit (an exception included) it
+// waits for the copies in flight, so none touches the caller's buffers after
+// the call returns.
+struct HostPipe {
+	cudaStream_t h2d = nullptr, comp = nullptr, d2h = nullptr;
+	cudaEvent_t in[2] = {}, done[2] = {}, out[2] = {}, shared = nullptr;
+	HostPipe()
+	{
+		check(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
+		check(cudaStreamCreateWithFlags(&comp, cudaStreamNonBlocking));
+		check(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+		for (int i = 0; i < 2; ++i) {
+			check(cudaEventCreateWithFlags(&in[i], cudaEventDisableTiming));
+			check(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
+			check(cudaEventCreateWithFlags(&out[i], cudaEventDisableTiming));
+		}
+		check(cudaEventCreateWithFlags(&shared, cudaEventDisableTiming));
+	}
+	~HostPipe()
+	{
+		for (cudaStream_t s : {h2d, comp, d2h})
+			if (s) {
+				cudaStreamSynchronize(s);
+				cudaStreamDestroy(s);
+			}
+		for (int i = 0; i < 2; ++i)
+			for (cudaEvent_t e : {in[i], done[i], out[i]})
+				if (e)
+					cudaEventDestroy(e);
+		if (shared)
+			cudaEventDestroy(shared);
+	}
+};
+
+static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_options &o,
+	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask)
+{
+	int dev;
+	check(cudaGetDevice(&dev));
+	const DeviceInfo di = device_info(dev);
+	// A host map used by more than one frame is shared: uploaded once.
+	std::map<const void *, int> uses;
+	auto model_map = [](const cusmic_image &im, const double *p) { return im.error ? nullptr : p; };
+	for (size_t f = 0; f < nf; ++f) {
+		const cusmic_image &im = ims[f];
+		for (const void *p : {(const void *)im.error, (const void *)model_map(im, im.gain),
+			     (const void *)model_map(im, im.readnoise), (const void *)im.background,
+			     (const void *)im.mask})
+			if (p)
+				++uses[p];
+	}
+	auto is_shared = [&](const void *p) { return p && uses[p] > 1; };
+	// Each shared map: its pixels (the largest frame that reads it), its
+	// check (validate_kernel's minimum and flag; mask: none) and its offset in
+	// the shared buffer of its type.
+	struct SharedMap {
+		size_t n = 0, off = 0;
+		int minimum = 0;
+		unsigned bit = 0; // 0: a mask
+	};
+	std::map<const void *, SharedMap> shared;
+	for (size_t f = 0; f < nf; ++f) {
+		const cusmic_image &im = ims[f];
+		const size_t n = im.width * im.height;
+		const struct {
+			const void *p;
+			int minimum;
+			unsigned bit;
+		} maps[] = {{im.error, 1, 1u}, {model_map(im, im.gain), 1, 2u},
+			{model_map(im, im.readnoise), 0, 4u}, {im.background, -1, 8u}, {im.mask, 0, 0u}};
+		for (const auto &m : maps)
+			if (is_shared(m.p)) {
+				SharedMap &e = shared[m.p];
+				e.n = std::max(e.n, n);
+				e.minimum = m.minimum;
+				e.bit = m.bit;
+			}
+	}
+	size_t shared_px = 0, shared_mask_px = 0;
+	for (auto &e : shared) {
+		size_t &end = e.second.bit ? shared_px : shared_mask_px;
+		e.second.off = end;
+		end += hb_round(e.second.n);
+	}
+	// Chunks of consecutive frames: input bytes up to HB_CHUNK_BYTES, at
+	// least one frame.
+	std::vector<size_t> first{0};
+	size_t bytes = 0, chunk_px = 0, max_px = 0;
+	for (size_t f = 0; f < nf; ++f) {
+		const cusmic_image &im = ims[f];
+		const size_t n = im.width * im.height;
+		size_t fb = 8 * n;
+		for (const double *p : {im.error, model_map(im, im.gain), model_map(im, im.readnoise),
+			     im.background})
+			fb += p && !is_shared(p) ? 8 * n : 0;
+		fb += im.mask && !is_shared(im.mask) ? n : 0;
+		if (f > first.back() && bytes + fb > HB_CHUNK_BYTES) {
+			first.push_back(f);
+			bytes = chunk_px = 0;
+		}
+		bytes += fb;
+		chunk_px += hb_round(n);
+		max_px = std::max(max_px, chunk_px);
+	}
+	first.push_back(nf);
+	const size_t nchunks = first.size() - 1;
+	std::vector<size_t> out_off(nf + 1, 0); // first output pixel of each frame
+	for (size_t f = 0; f < nf; ++f)
+		out_off[f + 1] = out_off[f] + ims[f].width * ims[f].height;
+
+	Lease wl[2] = {Lease(dev), Lease(dev)};
+	Workspace *ws[2] = {&*wl[0], &*wl[1]};
+	bool any[5] = {}; // per-frame (not shared) maps present: error, gain, rn, bg, mask
+	for (size_t f = 0; f < nf; ++f) {
+		const cusmic_image &im = ims[f];
+		any[0] |= im.error && !is_shared(im.error);
+		any[1] |= model_map(im, im.gain) && !is_shared(im.gain);
+		any[2] |= model_map(im, im.readnoise) && !is_shared(im.readnoise);
+		any[3] |= im.background && !is_shared(im.background);
+		any[4] |= im.mask && !is_shared(im.mask);
+	}
+	for (Workspace *w : ws) {
+		w->hdata.ensure(max_px);
+		w->hclean.ensure(max_px);
+		w->hout.ensure(max_px);
+		if (any[0])
+			w->herror.ensure(max_px);
+		if (any[1])
+			w->hgain.ensure(max_px);
+		if (any[2])
+			w->hrn.ensure(max_px);
+		if (any[3])
+			w->hbg.ensure(max_px);
+		if (any[4])
+			w->hmask.ensure(max_px);
+		w->hflags.ensure(1);
+		w->hflags_host.ensure(1);
+	}
+	if (shared_px)
+		ws[0]->hshared.ensure(shared_px);
+	if (shared_mask_px)
+		ws[0]->hshared_mask.ensure(shared_mask_px);
+	HostPipe pipe;
+	auto up = [&](Workspace &w, void *dst, const void *src, size_t n) {
+		if (HostStage::pinned(src))
+			check(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, pipe.h2d));
+		else
+			w.stage_io.in(dst, src, n, pipe.h2d);
+	};
+	auto validate = [&](const double *p, long long n, int minimum, unsigned *flags, unsigned bit) {
+		const long long blocks = (n + 255) / 256 < di.sms * 4 ? (n + 255) / 256 : di.sms * 4;
+		validate_kernel<<<(int)blocks, 256, 0, pipe.comp>>>(p, n, minimum, flags, bit);
+	};
+	// Shared maps first (on the inbound stream, ahead of every chunk).
+	for (const auto &e : shared) {
+		if (e.second.bit)
+			up(*ws[0], ws[0]->hshared.p + e.second.off, e.first, e.second.n * sizeof(double));
+		else
+			up(*ws[0], ws[0]->hshared_mask.p + e.second.off, e.first, e.second.n);
+	}
+	check(cudaEventRecord(pipe.shared, pipe.h2d));
+
+	std::vector<cusmic_image> dims(nf);
+	auto finish_chunk = [&](size_t k) {
+		Workspace &w = *ws[k & 1];
+		check(cudaEventSynchronize(pipe.done[k & 1]));
+		throw_map_flags(*w.hflags_host.p);
+		for (size_t f = first[k]; f < first[k + 1]; ++f)
+			check_state(w.hstate.p[f - first[k]]);
+		check(cudaStreamWaitEvent(pipe.d2h, pipe.done[k & 1], 0));
+		size_t off = 0;
+		for (size_t f = first[k]; f < first[k + 1]; ++f) {
+			const size_t n = ims[f].width * ims[f].height;
+			for (int part = 0; part < 2; ++part) {
+				void *dst = part ? (void *)(mask + out_off[f]) : (void *)(clean + out_off[f]);
+				const void *src = part ? (const void *)(w.hout.p + off) : (const void *)(w.hclean.p + off);
+				const size_t len = part ? n : n * sizeof(double);
+				if (HostStage::pinned(dst))
+					check(cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToHost, pipe.d2h));
+				else
+					w.stage_io.out(dst, src, len, pipe.d2h);
+			}
+			off += n;
+		}
+		check(cudaEventRecord(pipe.out[k & 1], pipe.d2h));
+	};
+	for (size_t k = 0; k < nchunks; ++k) {
+		Workspace &w = *ws[k & 1];
+		const size_t f0 = first[k], f1 = first[k + 1], nc = f1 - f0;
+		// Inputs of the chunk (its slot's last reader, chunk k - 2, finished:
+		// the host waited for it before issuing chunk k - 1's outbound copy).
+		size_t off = 0;
+		for (size_t f = f0; f < f1; ++f) {
+			const cusmic_image &im = ims[f];
+			const size_t n = im.width * im.height;
+			cusmic_image &d = dims[f];
+			d = im;
+			d.data = w.hdata.p + off;
+			up(w, w.hdata.p + off, im.data, n * sizeof(double));
+			auto place = [&](const double *p, DevBuf<double> &b) -> const double * {
+				if (!p)
+					return nullptr;
+				if (is_shared(p))
+					return ws[0]->hshared.p + shared[p].off;
+				up(w, b.p + off, p, n * sizeof(double));
+				return b.p + off;
+			};
+			d.error = place(im.error, w.herror);
+			d.gain = place(model_map(im, im.gain), w.hgain);
+			d.readnoise = place(model_map(im, im.readnoise), w.hrn);
+			d.background = place(im.background, w.hbg);
+			if (im.mask) {
+				if (is_shared(im.mask)) {
+					d.mask = ws[0]->hshared_mask.p + shared[im.mask].off;
+				} else {
+					up(w, w.hmask.p + off, im.mask, n);
+					d.mask = w.hmask.p + off;
+				}
+			}
+			off += hb_round(n);
+		}
+		check(cudaEventRecord(pipe.in[k & 1], pipe.h2d));
+		// Clean the chunk once its inputs are up and its slot's outputs of
+		// chunk k - 2 are down.
+		check(cudaStreamWaitEvent(pipe.comp, pipe.in[k & 1], 0));
+		if (k >= 2)
+			check(cudaStreamWaitEvent(pipe.comp, pipe.out[k & 1], 0));
+		check(cudaMemsetAsync(w.hflags.p, 0, sizeof(unsigned), pipe.comp));
+		if (k == 0) { // the shared maps are checked with the first chunk
+			check(cudaStreamWaitEvent(pipe.comp, pipe.shared, 0));
+			for (const auto &e : shared)
+				if (e.second.bit)
+					validate(ws[0]->hshared.p + e.second.off, (long long)e.second.n,
+						e.second.minimum, w.hflags.p, e.second.bit);
+		}
+		for (size_t f = f0; f < f1; ++f) {
+			const cusmic_image &im = ims[f], &d = dims[f];
+			const long long n = (long long)(im.width * im.height);
+			if (im.error && !is_shared(im.error))
+				validate(d.error, n, 1, w.hflags.p, 1u);
+			if (d.gain && !is_shared(im.gain))
+				validate(d.gain, n, 1, w.hflags.p, 2u);
+			if (d.readnoise && !is_shared(im.readnoise))
+				validate(d.readnoise, n, 0, w.hflags.p, 4u);
+			if (im.background && !is_shared(im.background))
+				validate(d.background, n, -1, w.hflags.p, 8u);
+		}
+		Layout L = make_layout(dims.data() + f0, nc, o, sc ? sc + f0 : nullptr, w.hclean.p,
+			w.hout.p, di);
+		upload(w, L, pipe.comp);
+		enqueue_plain(w, L, di, pipe.comp);
+		w.hstate.ensure(nc);
+		check(cudaMemcpyAsync(w.hstate.p, w.state.p, nc * sizeof(FrameState), cudaMemcpyDeviceToHost,
+			pipe.comp));
+		check(cudaMemcpyAsync(w.hflags_host.p, w.hflags.p, sizeof(unsigned), cudaMemcpyDeviceToHost,
+			pipe.comp));
+		check(cudaEventRecord(pipe.done[k & 1], pipe.comp));
+		if (k >= 1)
+			finish_chunk(k - 1);
+	}
+	finish_chunk(nchunks - 1);
+	check(cudaStreamSynchronize(pipe.d2h));
+	check(cudaGetLastError());
+}
+
+} // namespace cb
+
+extern "C" int cusmic_batch_host(const cusmic_image *ims, size_t nf, const cusmic_options *o,
+	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask, char *msg, size_t len)
+{
+	return guarded([&] {
+		check_arguments(ims, nf, o, sc, clean, mask, false);
+		run_host_batch(ims, nf, *o, sc, clean, mask);
 	}, msg, len);
 }
 
@@ -1334,15 +1672,16 @@ extern "C" int cusmic_plan_backward(cusmic_plan *p, const double *grad_clean, do
 // Allocation-free single-frame entry point.
 //
 // Some callers cannot allocate device memory at the moment they clean a frame:
-// a pipeline that is being captured into a CUDA graph (cudaMalloc/cudaFree are
-// not stream-ordered and cudaFree synchronises the device), a real-time
-// acquisition loop that forbids allocation after start-up, or a process whose
-// caching allocator has already reserved the device.  For them this entry
-// point keeps all of its scratch (descriptor, per-frame state, loop control,
-// work lists, bit planes and target/candidate/seed lists) in the static
-// device array below.  Every GPU that loads this library holds the array until
-// the process exits.  Calls share it: two calls whose work overlaps on the GPU
-// race, so callers serialise them (one stream, or their own ordering).
+// a real-time acquisition loop that allows allocation only at start-up
+// (cudaMalloc can block for milliseconds and cudaFree synchronises the whole
+// device), or a process whose own caching allocator has already reserved the
+// GPU's memory, so a cudaMalloc here would fail.  For them this entry point
+// keeps all of its scratch (descriptor, per-frame state, loop control, work
+// lists, bit planes and target/candidate/seed lists) in the static device
+// array below.  Every GPU that loads this library holds the array until the
+// process exits.  Calls share it and it keeps the last call's contents, so
+// every call clears what must start at zero; two calls whose work overlaps on
+// the GPU race, so callers serialise them (one stream, or their own ordering).
 
 namespace cb {
 
@@ -1456,6 +1795,21 @@ extern "C" int cusmic_set_tuning(const cusmic_tuning *table, size_t n, char *msg
 	}, msg, len);
 }
 
+extern "C" int cusmic_inject_fault(int what, long long value)
+{
+	switch (what) {
+	case CUSMIC_FAULT_PREPARE_WAIT:
+	case CUSMIC_FAULT_DETECT_WAIT:
+		inject_wait[what - CUSMIC_FAULT_PREPARE_WAIT].store(value > 0 ? value : 0);
+		return CUSMIC_OK;
+	case CUSMIC_FAULT_NO_MEMORY:
+		inject_alloc_failures.store(value > 0 ? value : 0);
+		return CUSMIC_OK;
+	default:
+		return CUSMIC_INVALID;
+	}
+}
+
 extern "C" int cusmic_get_tuning(size_t total_pixels, cusmic_tuning *out)
 {
 	if (!out)
@@ -1469,6 +1823,7 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 {
 	return guarded([&] {
 		check_arguments(im, 1, o, nullptr, clean, mask, true);
+		check_device_alignment(im, 1, clean);
 		if (im->width * im->height > NOALLOC_MAX_PIXELS || im->height > (size_t)NOALLOC_MAX_ROWS)
 			throw InvalidArgument("frame exceeds the static scratch: at most 262144 pixels "
 				"and 16384 rows");

@@ -89,7 +89,7 @@ validate_kernel(const double *__restrict__ v, long long n, int minimum, unsigned
 }
 
 __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
-	unsigned long long cand_cap)
+	unsigned long long cand_cap, long long poison_prepare = 0, long long poison_detect = 0)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < nf) {
@@ -102,6 +102,8 @@ __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter
 		c.maxiter = maxiter;
 		c.cand_cap = cand_cap;
 		c.any_active = maxiter > 0;
+		c.poison_wait[0] = poison_prepare;
+		c.poison_wait[1] = poison_detect;
 		*ctl = c;
 	}
 }

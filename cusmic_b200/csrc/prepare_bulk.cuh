@@ -37,6 +37,8 @@ struct __align__(128) PrepStage {
 	unsigned long long full[2]; // completion of each buffer's copies
 };
 
+// The warps' stages, then the block's abort word and (8 bytes further) the
+// barrier of an injected failure.
 constexpr size_t PB_SMEM = PB_WARPS * sizeof(PrepStage) + 16;
 
 // The frames prepare_bulk_kernel serves.
@@ -94,10 +96,14 @@ prepare_bulk_kernel(const FrameDesc *__restrict__ frames, FrameState *state, con
 	extern __shared__ __align__(128) unsigned char pb_smem[];
 	PrepStage *stages = reinterpret_cast<PrepStage *>(pb_smem);
 	int *abort = reinterpret_cast<int *>(pb_smem + PB_WARPS * sizeof(PrepStage));
+	unsigned long long *poison =
+		reinterpret_cast<unsigned long long *>(pb_smem + PB_WARPS * sizeof(PrepStage) + 8);
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	PrepStage &S = stages[warp];
-	if (threadIdx.x == 0)
+	if (threadIdx.x == 0) {
 		*abort = 0;
+		mbar_init(poison, 1);
+	}
 	if (lane == 0) {
 		mbar_init(&S.full[0], 1);
 		mbar_init(&S.full[1], 1);
@@ -117,7 +123,9 @@ prepare_bulk_kernel(const FrameDesc *__restrict__ frames, FrameState *state, con
 	uint32_t any_hole = 0, any_allowed = 0, any_finite = 0;
 	int ndonor = 0;
 	bool ok = true;
-	for (int i = 0; seg_valid(proc, nrows); ++i) {
+	if (warp == 0 && blockIdx.x == 0 && ctl->poison_wait[0] > 0) // injected failure
+		ok = __all_sync(0xffffffffu, poisoned_wait(poison, abort, ctl->poison_wait[0]));
+	for (int i = 0; ok && seg_valid(proc, nrows); ++i) {
 		const int b = i & 1;
 		ok = __all_sync(0xffffffffu, mbar_wait(&S.full[b], (i >> 1) & 1, abort));
 		if (!ok)

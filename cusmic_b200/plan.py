@@ -151,6 +151,18 @@ class Plan:
             o.background = math.nan if b is None else b
         return o
 
+    def bind(self, batch):
+        """Point the plan at another batch of the same shapes and maps (same
+        sharing of error maps): the workspace, tile lists and graph are kept,
+        only the frame descriptors are uploaded again."""
+        ims = batch.images()
+        msg = ctypes.create_string_buffer(256)
+        with torch.cuda.device(batch.device):
+            st = _native.lib().cusmic_plan_bind(self.handle, ims, batch.clean.data_ptr(),
+                                                batch.mask_out.data_ptr(), msg, 256)
+        _native.raise_for(st, msg)
+        self.batch, self._ims = batch, ims
+
     def _stream(self, stream):
         if stream is None:
             stream = torch.cuda.current_stream(self.batch.device)

@@ -43,6 +43,24 @@ cusmic_ragged_batch_device(const struct cusmic_image *ims, size_t nf,
 	const struct cusmic_options *options, const struct cusmic_frame_scalars *scalars,
 	double *clean, uint8_t *mask, void *stream, char *msg, size_t message_size);
 
+/* Ragged batch of 1..65535 frames in HOST memory, results into host memory
+ * (frame f's outputs at offset sum_{g<f} width_g * height_g of clean and
+ * mask).  Frames are cleaned on the current device in chunks of whole frames
+ * with the copies of neighbouring chunks overlapped: chunk k + 1's inputs go
+ * up while chunk k is cleaned and chunk k - 1's results come down.  A map
+ * pointer that several frames share is uploaded and checked once.  Map
+ * contents are checked like remove_cosmics's (same messages).  Page-locked
+ * buffers are copied by DMA directly; pageable ones through pinned staging
+ * (correct, without the overlap).  On failure, frames of the chunks before the
+ * failing one hold their results and the later frames' outputs are unchanged.
+ * Returns after the last result has landed.  No counterpart in the reference,
+ * whose host entry point takes one frame (src/api.cu:155-175); this is that
+ * call for a batch, with remove_cosmics's status and message rules. */
+int
+cusmic_batch_host(const struct cusmic_image *ims, size_t nf, const struct cusmic_options *options,
+	const struct cusmic_frame_scalars *scalars, double *clean, uint8_t *mask, char *msg,
+	size_t message_size);
+
 typedef struct cusmic_plan cusmic_plan;
 
 /* Plan flags. */
@@ -138,21 +156,47 @@ int
 cusmic_get_tuning(size_t total_pixels, struct cusmic_tuning *out);
 
 /* remove_cosmics_device for callers that cannot allocate device memory when
- * they clean a frame: code being captured into a CUDA graph (cudaMalloc and
- * cudaFree are not stream-ordered; cudaFree synchronises the device), real-time
- * loops that forbid allocation after start-up, or processes whose allocator
- * has already reserved the GPU.  Same arguments and results as
- * remove_cosmics_device, for one frame of at most 262144 pixels and 16384 rows
- * (larger frames are rejected with CUSMIC_INVALID).  All scratch lives in a
- * 12 MiB static device array that every GPU loading this library holds until
- * the process exits; the call allocates nothing.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress), so make that
- * first call before any stream capture.  Calls share the array: calls whose
- * work overlaps on the GPU race, so serialise them.  Synchronises before
- * returning.  No counterpart in the reference. */
+ * they clean a frame: real-time acquisition loops that allow allocation only
+ * at start-up (cudaMalloc can block for milliseconds and cudaFree synchronises
+ * the whole device), and processes whose own caching allocator has already
+ * reserved the GPU's memory, so that a cudaMalloc of this library's scratch
+ * would fail.  Same arguments and results as remove_cosmics_device, for one
+ * frame of at most 262144 pixels and 16384 rows (larger frames are rejected
+ * with CUSMIC_INVALID).  All scratch lives in a 12 MiB static device array
+ * that every GPU loading this library holds until the process exits; the call
+ * allocates nothing.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  Calls share the array, which keeps the last call's contents:
+ * calls whose work overlaps on the GPU race, so serialise them (one stream,
+ * or the caller's own ordering).  Synchronises before returning.  No
+ * counterpart in the reference. */
 int
 remove_cosmics_device_noalloc(const struct cusmic_image *image, const struct cusmic_options *options,
 	double *clean, uint8_t *mask, void *stream, char *msg, size_t message_size);
+
+/* Failures injected for tests of the error paths; none is in force unless a
+ * caller sets it.  No counterpart in the reference, whose tests inject none.
+ *
+ *   CUSMIC_FAULT_PREPARE_WAIT, CUSMIC_FAULT_DETECT_WAIT: value > 0 makes one
+ *     warp of the bulk-staged prepare kernel, or of the dense detection
+ *     kernel, wait up to `value` SM cycles on a barrier that nothing
+ *     completes, in calls (and plans) laid out after this call.  The wait
+ *     runs out like a wait whose copies never land: the kernel drains its
+ *     copies in flight, the loop control stops every frame and the call
+ *     returns CUSMIC_CUDA_ERROR.  value <= 0 removes the injection.
+ *   CUSMIC_FAULT_NO_MEMORY: the next `value` workspace reservations fail as
+ *     an exhausted cudaMalloc would (CUSMIC_NO_MEMORY; the host entry point
+ *     leaves its outputs unchanged).
+ *
+ * Returns CUSMIC_INVALID for an unknown kind. */
+enum cusmic_fault {
+	CUSMIC_FAULT_PREPARE_WAIT = 1,
+	CUSMIC_FAULT_DETECT_WAIT = 2,
+	CUSMIC_FAULT_NO_MEMORY = 3
+};
+
+int
+cusmic_inject_fault(int what, long long value);
 
 #ifdef __cplusplus
 }

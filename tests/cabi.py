@@ -33,6 +33,7 @@ class Frames:
 
     def __init__(self, frames, device="cuda"):
         self.keep = []
+        self.uploaded = {}  # id of a host array -> its device copy (shared maps stay shared)
         self.frames = frames
         self.nf = len(frames)
         self.ims = (_native.Image * self.nf)()
@@ -54,8 +55,12 @@ class Frames:
         self.mask = torch.empty(self.total, dtype=torch.uint8, device=device)
 
     def _dev(self, a, device):
+        hit = self.uploaded.get(id(a))
+        if hit is not None and hit[0] is a:
+            return hit[1]
         t = torch.from_numpy(np.ascontiguousarray(a)).to(device)
         self.keep.append(t)
+        self.uploaded[id(a)] = (a, t)  # keeps `a` alive, so its id is not reused
         return t
 
     def scalars(self):

@@ -141,3 +141,30 @@ def test_tuning_table_validation_and_lookup():
         assert (d["dense_rows"], d["dense_blocks_per_sm"]) == (0, 6)
     finally:
         _native.set_tuning(saved)
+
+
+def test_inject_fault_kinds():
+    """The failure-injection hook accepts its three kinds (each removed again
+    at once) and rejects any other."""
+    L = _native.lib()
+    for kind in (_native.FAULT_PREPARE_WAIT, _native.FAULT_DETECT_WAIT, _native.FAULT_NO_MEMORY):
+        assert L.cusmic_inject_fault(kind, 0) == _native.CUSMIC_OK
+    assert L.cusmic_inject_fault(0, 1) == _native.CUSMIC_INVALID
+    assert L.cusmic_inject_fault(99, 1) == _native.CUSMIC_INVALID
+
+
+def test_host_batch_argument_checks():
+    """cusmic_batch_host checks its arguments like the ragged device call,
+    before any copy or device call."""
+    L = _native.lib()
+    o = _native.default_options()
+    o.gain = 1.0
+    msg = ctypes.create_string_buffer(256)
+    assert L.cusmic_batch_host(None, 1, ctypes.byref(o), None, 8, 8, msg, 256) == \
+        _native.CUSMIC_INVALID
+    data = np.zeros(4)
+    im = _native.Image(data.ctypes.data, None, None, None, None, None, 2, 2)
+    o.cr_threshold = math.nan
+    assert L.cusmic_batch_host(ctypes.byref(im), 1, ctypes.byref(o), None, 8, 8, msg, 256) == \
+        _native.CUSMIC_INVALID
+    assert msg.value == b"invalid detection settings"
