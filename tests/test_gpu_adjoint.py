@@ -240,7 +240,9 @@ def test_autograd_reuses_plans(cuda):
         assert torch.equal(fresh_batch.clean.view(torch.int64), clean.detach().view(torch.int64))
         assert torch.equal(fresh_batch.mask_out.bool(), mask)
         gx, _ = fresh.backward(w)
-        assert torch.equal(gx, x.grad)
+        # The scatter adds with float64 atomics: the order of the additions,
+        # and so the last bits, may differ between two backwards.
+        assert torch.allclose(gx, x.grad, rtol=1e-13, atol=1e-13)
         fresh.close()
         if k == 1:  # keep this graph alive: its plan must not be handed out
             kept = (x, clean, mask, gx.clone())
@@ -250,4 +252,4 @@ def test_autograd_reuses_plans(cuda):
     x, clean, mask, g_kept = kept
     x.grad = None
     (w * clean).sum().backward()  # a second backward of the kept graph
-    assert torch.equal(x.grad, g_kept)
+    assert torch.allclose(x.grad, g_kept, rtol=1e-13, atol=1e-13)
