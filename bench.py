@@ -82,6 +82,12 @@ def parse_args():
     p.add_argument("--no-large", action="store_true", help="skip the 4 x 8192^2 forward/backward run")
     p.add_argument("--cpu-sample-rows", type=int, default=0,
                    help="rows of one frame timed for the CPU baseline (0: the whole frame)")
+    p.add_argument("--workload", choices=("stack_2048", "ragged_64"), default="stack_2048",
+                   help="ragged_64: time only the noise-model ragged batch (its first "
+                        "--ragged-frames frames), a short run for profiling its kernels")
+    p.add_argument("--ragged-frames", type=int, default=64)
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer runs")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     return p.parse_args()
 
 
@@ -270,6 +276,11 @@ def main():
         dist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                 timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.device("cuda", local)
+    if args.workload == "ragged_64":
+        ragged_only(args, world, rank, dev)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     sc = scenes.stack_2048(seed=rank, frames=args.frames, size=args.size)
     nf, h, w = args.frames, args.size, args.size
     total_px = nf * h * w
@@ -385,7 +396,8 @@ def main():
            "roofline": roofline, "roofline_sig_bulk": roofline_sig_bulk, "clocks": clk,
            "gpu_launches": launches_per_step * args.steps}
 
-    out["e2e"], out["e2e_per_frame"] = end_to_end(sc, plan, batch, args, world, barrier)
+    if not args.no_e2e:
+        out["e2e"], out["e2e_per_frame"] = end_to_end(sc, plan, batch, args, world, barrier)
 
     if not args.no_extras and world == 1:  # single-GPU comparisons
         out["plain"] = plain_vs_batched(plan, batch, stream, value / world, barrier)
@@ -399,7 +411,9 @@ def main():
         ragged_ctx["plan"].close()
         adjoint_ctx["plan"].close()
 
-    if rank == 0:
+    if rank == 0 and args.no_cpu:
+        print(json.dumps(out))
+    elif rank == 0:
         v, dt, n = cpu_reference(sc.frames[0].data, sc.error, sc.mask, args.cpu_sample_rows)
         out["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpix/s", "cores": os.cpu_count(),
                                "kind": "port",
@@ -411,6 +425,39 @@ def main():
     plan.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def ragged_only(args, world, rank, dev):
+    """The noise-model ragged batch (per-frame gain, read noise, background)
+    timed alone through a graph plan: a short run for profiling its kernels."""
+    import torch
+    from cusmic_b200 import _native, scenes
+    from cusmic_b200.plan import Plan, Batch
+    sc = scenes.ragged_64(seed=rank)
+    fr = sc.frames[:args.ragged_frames]
+    frames = [torch.from_numpy(f.data).to(dev) for f in fr]
+    batch = Batch.ragged(frames, scalars=[(f.gain, f.readnoise, f.background) for f in fr])
+    plan = Plan(batch, graph=True, **SETTINGS)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        plan.execute(stream)
+    plan.wait()
+    torch.cuda.synchronize(dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        plan.execute(stream)
+    e.record(stream)
+    e.synchronize()
+    plan.wait()
+    ms = s.elapsed_time(e) / args.steps
+    prof = plan.profile(stream)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "workload": f"ragged_64, first {len(fr)} frames",
+                          "value": round(batch.total / (ms / 1e3) / 1e6, 2), "unit": "Mpix/s",
+                          "ms_per_step": round(ms, 4), "steps": args.steps,
+                          "kernel_ms": {k: round(v, 4) for k, v in prof[0].items() if v}}))
+    plan.close()
 
 
 def end_to_end(sc, plan, batch, args, world, barrier):
@@ -468,12 +515,15 @@ def end_to_end(sc, plan, batch, args, world, barrier):
     v_frame = timed(frame_step, max(2, min(args.steps, 5)))
     same_frame = bool(torch.equal(h_flags.to(dev), batch.mask_out)) and bool(
         torch.equal(h_clean.to(dev).view(torch.int64), batch.clean.view(torch.int64)))
+    flagged = int(batch.mask_out.sum())
     e2e = {"value": round(v_batch, 2), "unit": "Mpix/s",
            "h2d_bytes_per_step": total_px * 8 + h * w * (8 + 1),
-           "d2h_bytes_per_step": total_px * (8 + 1),
+           "d2h_bytes_per_step": flagged * 16,
            "path": "cusmic_batch_host (host C ABI, whole stack per call: chunks of frames, "
-                   "inbound copy, cleaning and outbound copy of neighbouring chunks "
-                   "overlapped; shared error map and mask uploaded once), pinned buffers",
+                   "inbound copy and cleaning of neighbouring chunks overlapped; shared error "
+                   "map and mask uploaded once; no background, so each chunk returns its "
+                   "flagged pixels' positions and values (16 B each) and host threads copy "
+                   "the inputs to the outputs), pinned buffers",
            "identical_to_resident": same_batch}
     per_frame = {"value": round(v_frame, 2), "unit": "Mpix/s",
                  "h2d_bytes_per_step": total_px * (8 + 8 + 1),

@@ -386,7 +386,7 @@ sig_model_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restr
 
 // Noise model at an in-frame pixel (exact: its own 5 x 5 median of clean
 // under the border mode).
-__device__ __forceinline__ double noise_model_at(const FrameDesc &fd, int x, int y, int mode)
+__device__ __noinline__ double noise_model_at(const FrameDesc &fd, int x, int y, int mode)
 {
 	double v[25];
 #pragma unroll
@@ -453,9 +453,68 @@ __device__ __forceinline__ bool serves(const FrameDesc &fd)
 	return PATH == PATH_ANY || (fd.error != nullptr) == (PATH == PATH_ERROR);
 }
 
+// Scratch doubles per warp that candidate_sig needs: the sorted vertical runs
+// of the 9 x 9 patch on noise-model frames (CS_RUNS), else only the 25 window
+// values of the NaN rule.
+constexpr int CS_RUNS = 225;
+
+// The 25 noise medians of a staged candidate (src/filters.cuh:46-70, the
+// median<5> that noise_model reads), lane l < 25 returning the median of the
+// 5 x 5 block of the 9 x 9 patch P at rows l / 5 .. + 4, columns l % 5 .. + 4
+// (the window of window cell l).  Clean pixels are never NaN, so the middle
+// order statistic is the reference's value (its sign of a zero aside, which
+// max(m, 1e-5) removes).
+//
+// The 25 blocks share their columns: the 45 vertical runs of five (9 columns
+// x 5 row offsets) are sorted once per warp into S (S[(r * 5 + i) * 9 + c] =
+// i-th smallest of rows r .. r + 4 of column c).  A block of five sorted
+// columns whose rows are then sorted is sorted both ways, and its median is the
+// median of the 13 cells (i, j) with (i + 1)(j + 1) <= 13 and
+// (5 - i)(5 - j) <= 13: every other cell has at least 13 cells known to be no
+// larger (or no smaller) than it, six on each side.  So a lane sorts only the
+// rank rows of its five columns and takes a median of 13.
+__device__ __forceinline__ double patch_window_median(const double *P, double *S)
+{
+	const int lane = threadIdx.x & 31;
+	for (int k = lane; k < 45; k += 32) {
+		const int r = k / 9, c = k % 9;
+		const double *p = P + r * 9 + c;
+		double a = p[0], b = p[9], d = p[18], e = p[27], f = p[36];
+		sort5(a, b, d, e, f);
+		double *s = S + r * 45 + c;
+		s[0] = a;
+		s[9] = b;
+		s[18] = d;
+		s[27] = e;
+		s[36] = f;
+	}
+	__syncwarp();
+	double med = 0;
+	if (lane < 25) {
+		const double *R = S + (lane / 5) * 45 + lane % 5; // rank row i at R + 9 i, columns 0..4
+		double band[13];
+		int nb = 0;
+#pragma unroll
+		for (int i = 0; i < 5; ++i) {
+			double a = R[9 * i], b = R[9 * i + 1], c = R[9 * i + 2], d = R[9 * i + 3], e = R[9 * i + 4];
+			sort5(a, b, c, d, e);
+			const double row[5] = {a, b, c, d, e};
+#pragma unroll
+			for (int j = 0; j < 5; ++j)
+				if ((i + 1) * (j + 1) <= 13 && (5 - i) * (5 - j) <= 13)
+					band[nb++] = row[j];
+		}
+		med = median_network(band);
+	}
+	__syncwarp();
+	return med;
+}
+
+// S: the warp's scratch of at least CS_RUNS doubles on noise-model frames
+// (25 otherwise).
 template <bool LOW, int PATH = PATH_ANY>
 __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int y, double *P,
-	const DetectParams &prm, double &nz_center_out, bool fresh, bool skip = false)
+	double *S, const DetectParams &prm, double &nz_center_out, bool fresh, bool skip = false)
 {
 	const int lane = threadIdx.x & 31;
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
@@ -469,19 +528,14 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 		if (lane < 25 && err) // loads with the patch
 			nz = fd.error[(long long)(y + lane / 5 - 2) * w + x + lane % 5 - 2];
 		__syncwarp();
+		const int dy = lane / 5, dx = lane % 5;
+		if (!err) { // warp-uniform
+			const double m = patch_window_median(P, S);
+			if (lane < 25)
+				nz = noise_from_median(fd, (long long)(y + dy - 2) * w + x + dx - 2, m);
+		}
 		if (lane < 25) {
-			const int dy = lane / 5, dx = lane % 5;
 			const double *q = P + (dy + 2) * 9 + dx + 2; // the window cell
-			if (!err) {
-				const long long i = (long long)(y + dy - 2) * w + x + dx - 2;
-				double win[25];
-#pragma unroll
-				for (int a = 0; a < 5; ++a)
-#pragma unroll
-					for (int b = 0; b < 5; ++b)
-						win[a * 5 + b] = q[(a - 2) * 9 + b - 2];
-				nz = noise_from_median(fd, i, median_network(win));
-			}
 			v = lap_formula(q[0], q[-9], q[9], q[-1], q[1]) / (2 * nz);
 		}
 	} else if (lane < 25) {
@@ -501,12 +555,15 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 	const double nz_center = __shfl_sync(0xffffffffu, nz, 12);
 	double med;
 	if (__any_sync(0xffffffffu, isnan(v))) {
-		double win[25];
-#pragma unroll
-		for (int i = 0; i < 25; ++i)
-			win[i] = __shfl_sync(0xffffffffu, v, i);
-		med = lane == 0 ? window_median_exact(win, 25) : 0.0;
+		// The reference's NaN rule on the 25 values, in the warp's scratch
+		// (a register array indexed at run time would live in local memory).
+		__syncwarp();
+		if (lane < 25)
+			S[lane] = v;
+		__syncwarp();
+		med = lane == 0 ? window_median_exact(S, 25) : 0.0;
 		med = __shfl_sync(0xffffffffu, med, 0);
+		__syncwarp();
 	} else {
 		med = __shfl_sync(0xffffffffu, warp_sort32(v), 12);
 	}
@@ -529,13 +586,13 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 // is loaded before the evaluation and only read after it.
 template <bool LOW, int PATH = PATH_ANY>
 __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, long long e, int x, int y,
-	double *P, const DetectParams &prm, Seed *seeds, bool fresh, bool hole = false)
+	double *P, double *S, const DetectParams &prm, Seed *seeds, bool fresh, bool hole = false)
 {
 	double nz;
 	const long long word = (long long)y * fd.words + (x >> 5);
 	const uint32_t bit = 1u << (x & 31);
 	const uint32_t excl = LOW ? 0u : plane_ptr(fd, P_EXCL)[word];
-	const double sig = candidate_sig<LOW, PATH>(fd, x, y, P, prm, nz, fresh, hole);
+	const double sig = candidate_sig<LOW, PATH>(fd, x, y, P, S, prm, nz, fresh, hole);
 	if (!LOW && (threadIdx.x & 31) == 0) {
 		const bool seed = !hole && sig > prm.cr && !(excl & bit);
 		seeds[e] = seed ? Seed{t.x, t.y, sig, nz} : Seed{NO_SEED, 0, 0.0, 0.0};
@@ -555,7 +612,8 @@ candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 	DetectParams prm, Control *ctl, Seed *seeds, int fresh)
 {
 	__shared__ double patches[8][81];
-	double *P = patches[threadIdx.x >> 5];
+	__shared__ double scratch[8][CS_RUNS];
+	double *P = patches[threadIdx.x >> 5], *S = scratch[threadIdx.x >> 5];
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)ctl->n_cand;
@@ -569,7 +627,7 @@ candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 			continue; // warp-uniform
 		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
 		const bool hole = test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
-		candidate_eval<false, PATH>(fd, t, e, x, y, P, prm, seeds, fresh != 0, hole);
+		candidate_eval<false, PATH>(fd, t, e, x, y, P, S, prm, seeds, fresh != 0, hole);
 	}
 }
 
@@ -583,8 +641,9 @@ candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restri
 	DetectParams prm, Control *ctl, int fresh)
 {
 	__shared__ double patches[8][81];
+	__shared__ double scratch[8][PATH == PATH_ERROR ? 25 : CS_RUNS];
 	const int lane = threadIdx.x & 31;
-	double *P = patches[threadIdx.x >> 5];
+	double *P = patches[threadIdx.x >> 5], *S = scratch[threadIdx.x >> 5];
 	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
 	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = (long long)ctl->n_low;
@@ -614,7 +673,7 @@ candidate_low_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restri
 			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
 			const FrameDesc &fd = frames[tj.x];
 			candidate_eval<true, PATH>(fd, tj, base + j, (int)(tj.y % (unsigned)fd.w),
-				(int)(tj.y / (unsigned)fd.w), P, prm, nullptr, fresh != 0);
+				(int)(tj.y / (unsigned)fd.w), P, S, prm, nullptr, fresh != 0);
 		}
 	}
 }
@@ -761,6 +820,9 @@ __global__ void __launch_bounds__(256, PATH == PATH_ERROR ? 4 : 3)
 candidate_seed_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
 	DetectParams prm, Control *ctl, Seed *seeds, int fresh)
 {
+	// Error-map frames only: the scratch of candidate_sig holds just the 25
+	// values of the NaN rule, and the triples of the seed test serve as it.
+	static_assert(PATH == PATH_ERROR, "noise-model candidates run candidate_high_kernel");
 	__shared__ double patches[8][81];
 	__shared__ double triples[8][3][63];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -784,7 +846,8 @@ candidate_seed_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 		if (seeds && lane == 0)
 			seeds[e] = Seed{NO_SEED, 0, 0.0, 0.0};
 		double nz;
-		const double sig = candidate_sig<false, PATH>(fd, x, y, P, prm, nz, fresh != 0, hole);
+		const double sig = candidate_sig<false, PATH>(fd, x, y, P, &triples[warp][0][0], prm, nz,
+			fresh != 0, hole);
 		// Every lane holds the same sig, so the branch is warp-uniform.
 		if (!hole && sig > prm.cr && !(excl & bit))
 			seed_eval(fd, x, y, sig, nz, prm, P, triples[warp], fresh != 0, true);

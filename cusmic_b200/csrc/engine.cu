@@ -133,6 +133,8 @@ public:
 		return pool;
 	}
 
+	// memcpy(dst, src, n), or with src null memset(dst, 0, n), split over the
+	// workers and the calling thread.
 	void copy(void *dst, const void *src, size_t n)
 	{
 		const size_t parts = n >= (size_t(2) << 20) ? workers_.size() + 1 : 1;
@@ -141,23 +143,61 @@ public:
 		{
 			std::lock_guard<std::mutex> g(mu_);
 			for (size_t off = step; off < n; off += step) {
-				tasks_.push_back(Task{static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
-					std::min(step, n - off), &join});
+				tasks_.push_back(Task{static_cast<char *>(dst) + off,
+					src ? static_cast<const char *>(src) + off : nullptr, std::min(step, n - off), &join});
 				++join.left;
 			}
 		}
 		cv_.notify_all();
-		std::memcpy(dst, src, std::min(step, n));
+		part(dst, src, std::min(step, n));
 		std::unique_lock<std::mutex> lk(join.mu);
 		join.cv.wait(lk, [&] { return join.left == 0; });
 	}
 
-private:
+	// Parts of copies handed to the workers with submit(); wait() returns
+	// once all of them are done.  A Join must outlive its parts.
 	struct Join {
 		std::mutex mu;
 		std::condition_variable cv;
 		size_t left = 0;
 	};
+
+	// The same copy as copy(), split over the workers only, without waiting.
+	void submit(Join &join, void *dst, const void *src, size_t n)
+	{
+		if (workers_.empty() || !n) {
+			part(dst, src, n);
+			return;
+		}
+		const size_t parts = workers_.size();
+		const size_t step = ((n + parts - 1) / parts + 63) & ~size_t(63);
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			{
+				std::lock_guard<std::mutex> j(join.mu);
+				join.left += (n + step - 1) / step;
+			}
+			for (size_t off = 0; off < n; off += step)
+				tasks_.push_back(Task{static_cast<char *>(dst) + off,
+					src ? static_cast<const char *>(src) + off : nullptr, std::min(step, n - off), &join});
+		}
+		cv_.notify_all();
+	}
+
+	static void wait(Join &join)
+	{
+		std::unique_lock<std::mutex> lk(join.mu);
+		join.cv.wait(lk, [&] { return join.left == 0; });
+	}
+
+private:
+	static void part(void *dst, const void *src, size_t n)
+	{
+		if (src)
+			std::memcpy(dst, src, n);
+		else
+			std::memset(dst, 0, n);
+	}
 	struct Task {
 		char *dst;
 		const char *src;
@@ -196,7 +236,7 @@ private:
 				t = tasks_.front();
 				tasks_.pop_front();
 			}
-			std::memcpy(t.dst, t.src, t.n);
+			part(t.dst, t.src, t.n);
 			std::lock_guard<std::mutex> g(t.join->mu);
 			if (--t.join->left == 0)
 				t.join->cv.notify_all();
@@ -397,6 +437,12 @@ struct Workspace {
 	DevBuf<double> hshared;
 	DevBuf<uint8_t> hshared_mask;
 	PinBuf<unsigned> hflags_host;
+	// Its sparse return: the cleaned values along the target list, the
+	// list's length, and pinned host copies of list and values.
+	DevBuf<double> hsp_val;
+	PinBuf<unsigned long long> hcount;
+	PinBuf<uint2> hsp_idx_host;
+	PinBuf<double> hsp_val_host;
 };
 
 static std::mutex pool_mu;
@@ -614,8 +660,20 @@ static int grid_for_rows(const DeviceInfo &di, size_t nrows, int blocks_per_sm =
 	return (int)(blocks < 1 ? 1 : blocks > cap ? cap : blocks);
 }
 
+// The device address of page-locked host memory (mapped into the device's
+// address space).
+static const void *host_device_ptr(const void *p)
+{
+	void *d = nullptr;
+	check(cudaHostGetDevicePointer(&d, const_cast<void *>(p), 0));
+	return d;
+}
+
 // Allocate the workspace for L and upload descriptors (stream-ordered).
-static void upload(Workspace &ws, Layout &L, cudaStream_t s)
+// `mapped`: a kernel reads them from the page-locked staging buffer, so the
+// upload does not queue behind large copies on the copy engine (the host
+// batch entry point keeps its inbound copies running while it cleans).
+static void upload(Workspace &ws, Layout &L, cudaStream_t s, bool mapped = false)
 {
 	const size_t nf = L.frames.size();
 	ws.frames.ensure(nf);
@@ -664,14 +722,25 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s)
 	for (const Part &q : parts)
 		total += (q.bytes + 15) & ~size_t(15);
 	ws.stage.ensure(total);
+	WordCopies wc{};
+	const unsigned char *dstage = mapped
+		? static_cast<const unsigned char *>(host_device_ptr(ws.stage.p)) : nullptr;
 	size_t at = 0;
 	for (const Part &q : parts) {
 		if (q.bytes) {
 			std::memcpy(ws.stage.p + at, q.src, q.bytes);
-			check(cudaMemcpyAsync(q.dst, ws.stage.p + at, q.bytes, cudaMemcpyHostToDevice, s));
+			if (mapped) {
+				static_assert(sizeof(FrameDesc) % 8 == 0 && sizeof(FloorJob) % 8 == 0, "8-byte parts");
+				wc.part[wc.n++] = WordCopy{reinterpret_cast<const unsigned long long *>(dstage + at),
+					static_cast<unsigned long long *>(q.dst), (long long)(q.bytes / 8)};
+			} else {
+				check(cudaMemcpyAsync(q.dst, ws.stage.p + at, q.bytes, cudaMemcpyHostToDevice, s));
+			}
 		}
 		at += (q.bytes + 15) & ~size_t(15);
 	}
+	if (mapped && wc.n)
+		word_copy_kernel<<<32, 256, 0, s>>>(wc);
 }
 
 struct GraphLoop {
@@ -828,21 +897,28 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	Recorder *rec = nullptr)
 {
 	const int nf = (int)L.frames.size(), nrows = (int)L.rows.size();
-	init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
-		(unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1]);
 	if (!L.maxiter) {
+		init_kernel<<<(nf + 255) / 256, 256, 0, s>>>(ws.state.p, nf, ws.ctl.p, L.maxiter,
+			(unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1]);
 		mark(rec, K_INIT);
 		copy_kernel<<<grid_for_rows(di, nrows), 256, 0, s>>>(ws.frames.p, ws.rows.p, nrows);
 		mark(rec, K_COPY);
 		return;
 	}
-	// Zero the bit planes after DONOR (prepare_kernel writes every word of
-	// HOLE, EXCL and DONOR) and both row-mark arrays: nothing else writes them
-	// before the first pass, which therefore clears nothing itself.
-	static_assert(P_HOLE == 0 && P_EXCL == 1 && P_DONOR == 2 && P_CRMASK == 3, "plane order");
-	check(cudaMemsetAsync(ws.bits.p + P_CRMASK * L.plane_words, 0,
-		(size_t)(N_PLANES - P_CRMASK) * L.plane_words * sizeof(uint32_t), s));
-	check(cudaMemsetAsync(ws.rowmarks.p, 0, 2 * (size_t)L.row_words * sizeof(uint32_t), s));
+	// The same launch zeroes the bit planes from CRMASK to CHG and both
+	// row-mark arrays: nothing else writes them before the first pass, which
+	// therefore clears nothing itself.  prepare writes every word of HOLE,
+	// EXCL and DONOR, and of ROWMIN on noise-model frames (the only frames
+	// whose ROWMIN is read).  Planes and row marks are padded to 16 bytes.
+	static_assert(P_HOLE == 0 && P_EXCL == 1 && P_DONOR == 2 && P_CRMASK == 3 &&
+		P_ROWMIN == N_PLANES - 1, "plane order");
+	const long long z16 = (long long)(P_ROWMIN - P_CRMASK) * L.plane_words / 4;
+	const long long r16 = 2 * L.row_words / 4;
+	const long long zb = (z16 + 255) / 256, fb = (nf + 255) / 256, zcap = (long long)di.sms * 8;
+	init_kernel<<<(int)std::max(fb, std::min(zb, zcap)), 256, 0, s>>>(ws.state.p, nf, ws.ctl.p,
+		L.maxiter, (unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1],
+		reinterpret_cast<uint4 *>(ws.bits.p + P_CRMASK * L.plane_words), z16,
+		reinterpret_cast<uint4 *>(ws.rowmarks.p), r16);
 	mark(rec, K_INIT); // the state and the zeroed planes
 	launch_prepare(ws, L, di, s);
 	mark(rec, K_PREPARE);
@@ -1088,7 +1164,7 @@ extern "C" int cusmic_ragged_batch_device(const cusmic_image *ims, size_t nf,
 
 namespace cb {
 
-constexpr size_t HB_CHUNK_BYTES = size_t(24) << 20; // input bytes a chunk aims for
+constexpr size_t HB_CHUNK_BYTES = size_t(64) << 20; // input bytes a chunk aims for
 constexpr size_t HB_ALIGN = 16;                     // pixels: chunk offsets stay 16-byte aligned
 
 static size_t hb_round(size_t n)
@@ -1115,14 +1191,16 @@ static void throw_map_flags(unsigned bad)
 // the call returns.
 struct HostPipe {
 	cudaStream_t h2d = nullptr, comp = nullptr, d2h = nullptr;
-	cudaEvent_t in[2] = {}, done[2] = {}, out[2] = {}, shared = nullptr;
-	HostPipe()
+	std::vector<cudaEvent_t> in; // per chunk: its inputs are on the device
+	cudaEvent_t done[2] = {}, out[2] = {}, shared = nullptr;
+	explicit HostPipe(size_t chunks) : in(chunks, nullptr)
 	{
 		check(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
 		check(cudaStreamCreateWithFlags(&comp, cudaStreamNonBlocking));
 		check(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+		for (cudaEvent_t &e : in)
+			check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 		for (int i = 0; i < 2; ++i) {
-			check(cudaEventCreateWithFlags(&in[i], cudaEventDisableTiming));
 			check(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
 			check(cudaEventCreateWithFlags(&out[i], cudaEventDisableTiming));
 		}
@@ -1135,12 +1213,28 @@ struct HostPipe {
 				cudaStreamSynchronize(s);
 				cudaStreamDestroy(s);
 			}
+		for (cudaEvent_t e : in)
+			if (e)
+				cudaEventDestroy(e);
 		for (int i = 0; i < 2; ++i)
-			for (cudaEvent_t e : {in[i], done[i], out[i]})
+			for (cudaEvent_t e : {done[i], out[i]})
 				if (e)
 					cudaEventDestroy(e);
 		if (shared)
 			cudaEventDestroy(shared);
+	}
+};
+
+// Host copies of a call running on the copy threads; waited for on every
+// exit, so none writes into the caller's buffers after the call returns.
+struct HostCopies {
+	std::vector<std::unique_ptr<CopyPool::Join>> join;
+	explicit HostCopies(size_t n) : join(n) {}
+	~HostCopies()
+	{
+		for (auto &j : join)
+			if (j)
+				CopyPool::wait(*j);
 	}
 };
 
@@ -1216,12 +1310,24 @@ static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_opti
 	}
 	first.push_back(nf);
 	const size_t nchunks = first.size() - 1;
+	// A chunk whose frames have no background returns sparsely: without a
+	// background every output pixel outside the mask equals its input bit
+	// for bit (prepare copies it, restore writes holes back), so host threads
+	// copy the inputs to the outputs and only the flagged pixels' values and
+	// positions cross PCIe (16 bytes per flagged pixel instead of 9 per
+	// pixel).
+	std::vector<char> sparse(nchunks, 1);
+	bool any_sparse = false;
+	for (size_t k = 0; k < nchunks; ++k) {
+		for (size_t f = first[k]; f < first[k + 1]; ++f)
+			if (ims[f].background || !std::isnan(scalars_for(o, sc, f).bg))
+				sparse[k] = 0;
+		any_sparse |= sparse[k] != 0;
+	}
 	std::vector<size_t> out_off(nf + 1, 0); // first output pixel of each frame
 	for (size_t f = 0; f < nf; ++f)
 		out_off[f + 1] = out_off[f] + ims[f].width * ims[f].height;
 
-	Lease wl[2] = {Lease(dev), Lease(dev)};
-	Workspace *ws[2] = {&*wl[0], &*wl[1]};
 	bool any[5] = {}; // per-frame (not shared) maps present: error, gain, rn, bg, mask
 	for (size_t f = 0; f < nf; ++f) {
 		const cusmic_image &im = ims[f];
@@ -1231,33 +1337,49 @@ static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_opti
 		any[3] |= im.background && !is_shared(im.background);
 		any[4] |= im.mask && !is_shared(im.mask);
 	}
+	// Inputs go through a device ring of `slots` chunk slots.  When the whole
+	// call's inputs fit a quarter of the free device memory (at most
+	// 16 GiB) the ring holds every chunk, and every inbound copy is queued at
+	// the start; otherwise a slot is refilled as soon as its chunk is cleaned.
+	const size_t px_bytes = 8 + 8 * (any[0] + any[1] + any[2] + any[3]) + any[4];
+	size_t free_b = 0, total_b = 0;
+	check(cudaMemGetInfo(&free_b, &total_b));
+	const size_t budget = std::min(free_b / 4, size_t(16) << 30);
+	const size_t slots = std::max<size_t>(2, std::min(nchunks, budget / std::max<size_t>(1, max_px * px_bytes)));
+	Lease wl[2] = {Lease(dev), Lease(dev)};
+	Workspace *ws[2] = {&*wl[0], &*wl[1]};
+	Workspace &ring = *ws[0]; // the input ring and the shared maps
+	ring.hdata.ensure(slots * max_px);
+	if (any[0])
+		ring.herror.ensure(slots * max_px);
+	if (any[1])
+		ring.hgain.ensure(slots * max_px);
+	if (any[2])
+		ring.hrn.ensure(slots * max_px);
+	if (any[3])
+		ring.hbg.ensure(slots * max_px);
+	if (any[4])
+		ring.hmask.ensure(slots * max_px);
 	for (Workspace *w : ws) {
-		w->hdata.ensure(max_px);
 		w->hclean.ensure(max_px);
 		w->hout.ensure(max_px);
-		if (any[0])
-			w->herror.ensure(max_px);
-		if (any[1])
-			w->hgain.ensure(max_px);
-		if (any[2])
-			w->hrn.ensure(max_px);
-		if (any[3])
-			w->hbg.ensure(max_px);
-		if (any[4])
-			w->hmask.ensure(max_px);
-		w->hflags.ensure(1);
-		w->hflags_host.ensure(1);
+		w->hflags.ensure(2); // one 8-byte word: the flags and padding
+		w->hflags_host.ensure(2);
+		w->hcount.ensure(1);
+		if (any_sparse && o.maxiter)
+			w->hsp_val.ensure(max_px);
 	}
 	if (shared_px)
-		ws[0]->hshared.ensure(shared_px);
+		ring.hshared.ensure(shared_px);
 	if (shared_mask_px)
-		ws[0]->hshared_mask.ensure(shared_mask_px);
-	HostPipe pipe;
-	auto up = [&](Workspace &w, void *dst, const void *src, size_t n) {
+		ring.hshared_mask.ensure(shared_mask_px);
+	HostPipe pipe(nchunks);
+	HostCopies host(nchunks);
+	auto up = [&](void *dst, const void *src, size_t n) {
 		if (HostStage::pinned(src))
 			check(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, pipe.h2d));
 		else
-			w.stage_io.in(dst, src, n, pipe.h2d);
+			ring.stage_io.in(dst, src, n, pipe.h2d);
 	};
 	auto validate = [&](const double *p, long long n, int minimum, unsigned *flags, unsigned bit) {
 		const long long blocks = (n + 255) / 256 < di.sms * 4 ? (n + 255) / 256 : di.sms * 4;
@@ -1266,13 +1388,59 @@ static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_opti
 	// Shared maps first (on the inbound stream, ahead of every chunk).
 	for (const auto &e : shared) {
 		if (e.second.bit)
-			up(*ws[0], ws[0]->hshared.p + e.second.off, e.first, e.second.n * sizeof(double));
+			up(ring.hshared.p + e.second.off, e.first, e.second.n * sizeof(double));
 		else
-			up(*ws[0], ws[0]->hshared_mask.p + e.second.off, e.first, e.second.n);
+			up(ring.hshared_mask.p + e.second.off, e.first, e.second.n);
 	}
 	check(cudaEventRecord(pipe.shared, pipe.h2d));
+	// The host side of the sparse chunks (outputs = inputs, masks zero) runs
+	// on the copy threads from the start, in chunk order.
+	for (size_t k = 0; k < nchunks; ++k)
+		if (sparse[k]) {
+			host.join[k].reset(new CopyPool::Join);
+			for (size_t f = first[k]; f < first[k + 1]; ++f) {
+				const size_t np = ims[f].width * ims[f].height;
+				if (clean + out_off[f] != ims[f].data)
+					CopyPool::get().submit(*host.join[k], clean + out_off[f], ims[f].data,
+						np * sizeof(double));
+				CopyPool::get().submit(*host.join[k], mask + out_off[f], nullptr, np);
+			}
+		}
 
 	std::vector<cusmic_image> dims(nf);
+	auto issue_inputs = [&](size_t k) {
+		size_t off = (k % slots) * max_px;
+		for (size_t f = first[k]; f < first[k + 1]; ++f) {
+			const cusmic_image &im = ims[f];
+			const size_t n = im.width * im.height;
+			cusmic_image &d = dims[f];
+			d = im;
+			d.data = ring.hdata.p + off;
+			up(ring.hdata.p + off, im.data, n * sizeof(double));
+			auto place = [&](const double *p, DevBuf<double> &b) -> const double * {
+				if (!p)
+					return nullptr;
+				if (is_shared(p))
+					return ring.hshared.p + shared[p].off;
+				up(b.p + off, p, n * sizeof(double));
+				return b.p + off;
+			};
+			d.error = place(im.error, ring.herror);
+			d.gain = place(model_map(im, im.gain), ring.hgain);
+			d.readnoise = place(model_map(im, im.readnoise), ring.hrn);
+			d.background = place(im.background, ring.hbg);
+			if (im.mask) {
+				if (is_shared(im.mask)) {
+					d.mask = ring.hshared_mask.p + shared[im.mask].off;
+				} else {
+					up(ring.hmask.p + off, im.mask, n);
+					d.mask = ring.hmask.p + off;
+				}
+			}
+			off += hb_round(n);
+		}
+		check(cudaEventRecord(pipe.in[k], pipe.h2d));
+	};
 	auto finish_chunk = [&](size_t k) {
 		Workspace &w = *ws[k & 1];
 		check(cudaEventSynchronize(pipe.done[k & 1]));
@@ -1280,6 +1448,27 @@ static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_opti
 		for (size_t f = first[k]; f < first[k + 1]; ++f)
 			check_state(w.hstate.p[f - first[k]]);
 		check(cudaStreamWaitEvent(pipe.d2h, pipe.done[k & 1], 0));
+		if (sparse[k]) {
+			const size_t n = o.maxiter ? (size_t)*w.hcount.p : 0;
+			if (n) {
+				w.hsp_idx_host.ensure(n);
+				w.hsp_val_host.ensure(n);
+				check(cudaMemcpyAsync(w.hsp_idx_host.p, w.targets.p, n * sizeof(uint2),
+					cudaMemcpyDeviceToHost, pipe.d2h));
+				check(cudaMemcpyAsync(w.hsp_val_host.p, w.hsp_val.p, n * sizeof(double),
+					cudaMemcpyDeviceToHost, pipe.d2h));
+			}
+			check(cudaEventRecord(pipe.out[k & 1], pipe.d2h));
+			CopyPool::wait(*host.join[k]); // outputs = inputs, masks zero
+			check(cudaEventSynchronize(pipe.out[k & 1]));
+			for (size_t i = 0; i < n; ++i) {
+				const uint2 t = w.hsp_idx_host.p[i];
+				const size_t at = out_off[first[k] + t.x] + t.y;
+				clean[at] = w.hsp_val_host.p[i];
+				mask[at] = 1;
+			}
+			return;
+		}
 		size_t off = 0;
 		for (size_t f = first[k]; f < first[k + 1]; ++f) {
 			const size_t n = ims[f].width * ims[f].height;
@@ -1296,53 +1485,22 @@ static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_opti
 		}
 		check(cudaEventRecord(pipe.out[k & 1], pipe.d2h));
 	};
+	for (size_t k = 0; k < std::min(slots, nchunks); ++k)
+		issue_inputs(k);
 	for (size_t k = 0; k < nchunks; ++k) {
 		Workspace &w = *ws[k & 1];
 		const size_t f0 = first[k], f1 = first[k + 1], nc = f1 - f0;
-		// Inputs of the chunk (its slot's last reader, chunk k - 2, finished:
-		// the host waited for it before issuing chunk k - 1's outbound copy).
-		size_t off = 0;
-		for (size_t f = f0; f < f1; ++f) {
-			const cusmic_image &im = ims[f];
-			const size_t n = im.width * im.height;
-			cusmic_image &d = dims[f];
-			d = im;
-			d.data = w.hdata.p + off;
-			up(w, w.hdata.p + off, im.data, n * sizeof(double));
-			auto place = [&](const double *p, DevBuf<double> &b) -> const double * {
-				if (!p)
-					return nullptr;
-				if (is_shared(p))
-					return ws[0]->hshared.p + shared[p].off;
-				up(w, b.p + off, p, n * sizeof(double));
-				return b.p + off;
-			};
-			d.error = place(im.error, w.herror);
-			d.gain = place(model_map(im, im.gain), w.hgain);
-			d.readnoise = place(model_map(im, im.readnoise), w.hrn);
-			d.background = place(im.background, w.hbg);
-			if (im.mask) {
-				if (is_shared(im.mask)) {
-					d.mask = ws[0]->hshared_mask.p + shared[im.mask].off;
-				} else {
-					up(w, w.hmask.p + off, im.mask, n);
-					d.mask = w.hmask.p + off;
-				}
-			}
-			off += hb_round(n);
-		}
-		check(cudaEventRecord(pipe.in[k & 1], pipe.h2d));
 		// Clean the chunk once its inputs are up and its slot's outputs of
 		// chunk k - 2 are down.
-		check(cudaStreamWaitEvent(pipe.comp, pipe.in[k & 1], 0));
+		check(cudaStreamWaitEvent(pipe.comp, pipe.in[k], 0));
 		if (k >= 2)
 			check(cudaStreamWaitEvent(pipe.comp, pipe.out[k & 1], 0));
-		check(cudaMemsetAsync(w.hflags.p, 0, sizeof(unsigned), pipe.comp));
+		check(cudaMemsetAsync(w.hflags.p, 0, 2 * sizeof(unsigned), pipe.comp));
 		if (k == 0) { // the shared maps are checked with the first chunk
 			check(cudaStreamWaitEvent(pipe.comp, pipe.shared, 0));
 			for (const auto &e : shared)
 				if (e.second.bit)
-					validate(ws[0]->hshared.p + e.second.off, (long long)e.second.n,
+					validate(ring.hshared.p + e.second.off, (long long)e.second.n,
 						e.second.minimum, w.hflags.p, e.second.bit);
 		}
 		for (size_t f = f0; f < f1; ++f) {
@@ -1359,16 +1517,32 @@ static void run_host_batch(const cusmic_image *ims, size_t nf, const cusmic_opti
 		}
 		Layout L = make_layout(dims.data() + f0, nc, o, sc ? sc + f0 : nullptr, w.hclean.p,
 			w.hout.p, di);
-		upload(w, L, pipe.comp);
+		upload(w, L, pipe.comp, true);
 		enqueue_plain(w, L, di, pipe.comp);
+		if (sparse[k] && o.maxiter)
+			gather_targets_kernel<<<di.sms * 4, 256, 0, pipe.comp>>>(w.frames.p, w.targets.p,
+				&w.ctl.p->n_targets, w.hsp_val.p);
+		// The chunk's status into page-locked memory, written by a kernel
+		// (a copy would queue behind the outbound copies of earlier chunks).
 		w.hstate.ensure(nc);
-		check(cudaMemcpyAsync(w.hstate.p, w.state.p, nc * sizeof(FrameState), cudaMemcpyDeviceToHost,
-			pipe.comp));
-		check(cudaMemcpyAsync(w.hflags_host.p, w.hflags.p, sizeof(unsigned), cudaMemcpyDeviceToHost,
-			pipe.comp));
+		static_assert(sizeof(FrameState) % 8 == 0, "8-byte words");
+		WordCopies st{};
+		st.part[0] = WordCopy{reinterpret_cast<const unsigned long long *>(w.state.p),
+			static_cast<unsigned long long *>(const_cast<void *>(host_device_ptr(w.hstate.p))),
+			(long long)(nc * sizeof(FrameState) / 8)};
+		st.part[1] = WordCopy{&w.ctl.p->n_targets,
+			static_cast<unsigned long long *>(const_cast<void *>(host_device_ptr(w.hcount.p))), 1};
+		st.part[2] = WordCopy{reinterpret_cast<const unsigned long long *>(w.hflags.p),
+			static_cast<unsigned long long *>(const_cast<void *>(host_device_ptr(w.hflags_host.p))), 1};
+		st.n = 3;
+		word_copy_kernel<<<1, 256, 0, pipe.comp>>>(st);
 		check(cudaEventRecord(pipe.done[k & 1], pipe.comp));
-		if (k >= 1)
+		if (k >= 1) {
 			finish_chunk(k - 1);
+			// Chunk k - 1 is cleaned: its input slot takes chunk k - 1 + slots.
+			if (k - 1 + slots < nchunks)
+				issue_inputs(k - 1 + slots);
+		}
 	}
 	finish_chunk(nchunks - 1);
 	check(cudaStreamSynchronize(pipe.d2h));

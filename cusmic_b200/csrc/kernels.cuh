@@ -88,9 +88,18 @@ validate_kernel(const double *__restrict__ v, long long n, int minimum, unsigned
 		atomicOr(flags, bit);
 }
 
+// Per-frame state and loop control of a call; with `zero`, also zeroes the n16
+// 16-byte words at zero (the bit planes that nothing writes before the first
+// pass, and the row marks) with a grid-stride loop of 16-byte stores.
 __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
-	unsigned long long cand_cap, long long poison_prepare = 0, long long poison_detect = 0)
+	unsigned long long cand_cap, long long poison_prepare = 0, long long poison_detect = 0,
+	uint4 *zero = nullptr, long long n16 = 0, uint4 *zero2 = nullptr, long long n16b = 0)
 {
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n16; j += stride)
+		zero[j] = make_uint4(0u, 0u, 0u, 0u);
+	for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n16b; j += stride)
+		zero2[j] = make_uint4(0u, 0u, 0u, 0u);
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < nf) {
 		FrameState s = {};
@@ -862,6 +871,45 @@ copy_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ rows,
 			fd.clean[i] = isfinite(d) ? v : d;
 			fd.mask_out[i] = 0;
 		}
+	}
+}
+
+// Up to four copies of 8-byte words between any memory the device can
+// address, page-locked host memory included (read or written over the bus by
+// the kernel itself, so no copy engine is involved).
+struct WordCopy {
+	const unsigned long long *src;
+	unsigned long long *dst;
+	long long n8;
+};
+
+struct WordCopies {
+	WordCopy part[5];
+	int n;
+};
+
+__global__ void __launch_bounds__(256)
+word_copy_kernel(WordCopies c)
+{
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (int k = 0; k < c.n; ++k)
+		for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.part[k].n8; i += stride)
+			c.part[k].dst[i] = c.part[k].src[i];
+}
+
+// The cleaned values of the listed targets (the cumulative mask as
+// {frame, pixel}): vals[i] = clean of target i.  Without a background every
+// other output pixel equals its input bit for bit, so these values and the
+// list are all of a frame's result that differs from its input.
+__global__ void __launch_bounds__(256)
+gather_targets_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ list,
+	const unsigned long long *count, double *vals)
+{
+	const unsigned long long n = *count, stride = (unsigned long long)gridDim.x * blockDim.x;
+	for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+	     i += stride) {
+		const uint2 t = list[i];
+		vals[i] = frames[t.x].clean[t.y];
 	}
 }
 

@@ -83,6 +83,21 @@ template <int N> CB_HD double median_network(double (&v)[N])
 	return v[N / 2];
 }
 
+// Ascending sort of five values with nine compare-exchanges (an optimal
+// network; checked by the 0-1 principle over all 32 binary inputs).
+CB_HD void sort5(double &a, double &b, double &c, double &d, double &e)
+{
+	cas(a, b);
+	cas(d, e);
+	cas(c, e);
+	cas(c, d);
+	cas(b, e);
+	cas(a, d);
+	cas(a, c);
+	cas(b, d);
+	cas(b, c);
+}
+
 // Median of a NaN-free 3 x 3 window in row-major order: sort the columns,
 // then the median is med3(max of minima, med3 of middles, min of maxima).
 CB_HD double median9(double a0, double a1, double a2, double a3, double a4, double a5,

@@ -45,17 +45,20 @@ cusmic_ragged_batch_device(const struct cusmic_image *ims, size_t nf,
 
 /* Ragged batch of 1..65535 frames in HOST memory, results into host memory
  * (frame f's outputs at offset sum_{g<f} width_g * height_g of clean and
- * mask).  Frames are cleaned on the current device in chunks of whole frames
- * with the copies of neighbouring chunks overlapped: chunk k + 1's inputs go
- * up while chunk k is cleaned and chunk k - 1's results come down.  A map
- * pointer that several frames share is uploaded and checked once.  Map
- * contents are checked like remove_cosmics's (same messages).  Page-locked
- * buffers are copied by DMA directly; pageable ones through pinned staging
- * (correct, without the overlap).  On failure, frames of the chunks before the
- * failing one hold their results and the later frames' outputs are unchanged.
- * Returns after the last result has landed.  No counterpart in the reference,
- * whose host entry point takes one frame (src/api.cu:155-175); this is that
- * call for a batch, with remove_cosmics's status and message rules. */
+ * mask).  Frames are cleaned on the current device in chunks of whole frames;
+ * the inbound copies of later chunks run while earlier chunks are cleaned
+ * (every chunk's inputs are queued at once when they fit a quarter of the
+ * free device memory).  A map pointer that several frames share is uploaded
+ * and checked once.  A chunk whose frames have no background returns only its
+ * flagged pixels (16 bytes each): the other output pixels equal the inputs bit
+ * for bit, and host threads copy them.  Map contents are checked like
+ * remove_cosmics's (same messages).  Page-locked buffers are copied by DMA
+ * directly; pageable ones through pinned staging (correct, with less overlap).
+ * On failure, frames of the chunks before the failing one hold their results
+ * and the other outputs are unspecified.  Returns after the last result has
+ * landed.  No counterpart in the reference, whose host entry point takes one
+ * frame (src/api.cu:155-175); this is that call for a batch, with
+ * remove_cosmics's status and message rules. */
 int
 cusmic_batch_host(const struct cusmic_image *ims, size_t nf, const struct cusmic_options *options,
 	const struct cusmic_frame_scalars *scalars, double *clean, uint8_t *mask, char *msg,
