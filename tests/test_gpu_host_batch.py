@@ -133,8 +133,13 @@ def test_host_batch_map_checks_and_donor_error(cuda):
     st, msg, _, _ = run_host(bad, opts, True)
     assert st == _native.CUSMIC_INVALID and msg == "read noise must be finite and nonnegative"
     # A frame without donors in a later chunk: the frames of earlier chunks
-    # hold their results (the others are unspecified).
-    ok = frames_of("shared")[:4]
+    # hold their results (the others are unspecified).  Chunks take whole
+    # frames up to 64 MB of inputs, so with 2048^2 frames (32 MB each; the
+    # shared maps are not counted) the first chunk is frames 0 and 1 and the
+    # failing frame falls into the second.
+    from cusmic_b200 import scenes
+    sc = scenes.stack_2048(seed=4, frames=4, size=2048)
+    ok = [dict(data=f.data, error=sc.error, mask=sc.mask) for f in sc.frames]
     data = np.full((7, 7), 10.0)
     data[3, 3] = 1000
     nodonor = dict(data=data, error=np.ones((7, 7)), mask=np.ones((7, 7), bool))
@@ -143,8 +148,7 @@ def test_host_batch_map_checks_and_donor_error(cuda):
     st, msg, clean, mask = run_host(batch, cabi.options(**SETTINGS), True)
     assert st == _native.CUSMIC_INVALID and "no finite replacement donors" in msg
     n = ok[0]["data"].size
-    dev = cabi.Frames(ok[:3])
+    dev = cabi.Frames(ok[:2])
     assert cabi.run_ragged(dev, cabi.options(**SETTINGS))[0] == 0
-    c3 = dev.clean.cpu().numpy()
-    assert_bits_equal(clean[:3 * n], c3)  # the first chunk (three 1024^2 frames)
-    np.testing.assert_array_equal(mask[:3 * n], dev.mask.cpu().numpy())
+    assert_bits_equal(clean[:2 * n], dev.clean.cpu().numpy())  # the first chunk
+    np.testing.assert_array_equal(mask[:2 * n], dev.mask.cpu().numpy())
