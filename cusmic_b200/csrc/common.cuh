@@ -97,6 +97,10 @@ struct FrameDesc {
 	const double *data, *error, *gain_map, *rn_map, *bg_map;
 	const uint8_t *mask;
 	double *clean;     // working pixels, restored in place into the output
+	double *out;       // output pixels: clean itself (null means the same), or for a frame
+	                   // with a background the caller's buffer while clean is a
+	                   // workspace buffer: prepare then writes every output pixel
+	                   // except the flagged ones, which restore writes
 	uint8_t *mask_out; // uint8 output mask
 	uint32_t *bits;    // N_PLANES planes of `plane` words
 	BlockFloor *floors; // the frame's block floors, row-major by block (null: none)

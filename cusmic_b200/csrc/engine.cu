@@ -397,10 +397,11 @@ static DeviceInfo device_info(int dev)
 	DeviceInfo &d = cache[dev];
 	if (!d.sms) { // first use on this (the current) device
 		check(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
-		check(cudaFuncSetAttribute(prepare_bulk_kernel<false>,
-			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
-		check(cudaFuncSetAttribute(prepare_bulk_kernel<true>,
-			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
+		for (const void *k : {(const void *)prepare_bulk_kernel<false, false>,
+			     (const void *)prepare_bulk_kernel<true, false>,
+			     (const void *)prepare_bulk_kernel<false, true>,
+			     (const void *)prepare_bulk_kernel<true, true>})
+			check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
 	}
 	return d;
 }
@@ -417,6 +418,7 @@ struct Workspace {
 	DevBuf<int2> dirty;     // dirty-row list of an incremental pass
 	DevBuf<unsigned> sel;   // targets the replacement after a pass visits
 	DevBuf<Seed> seeds;     // seed slots of the noise-model candidates
+	DevBuf<double> work;    // working pixels of the frames with a background
 	DevBuf<uint2> cands;
 	DevBuf<int4> bulk;
 	DevBuf<FloorJob> jobs;
@@ -697,11 +699,23 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s, bool mapped = false
 		ws.pre.ensure(L.bulk.size() * BK_CWARPS * (size_t)BK_REGION);
 		ws.pre_counts.ensure(L.bulk.size() * BK_CWARPS);
 	}
+	// A frame with a background keeps its working pixels (data + background)
+	// in the workspace, and prepare writes its output pixels at once (the
+	// reference's (x + bg) - bg), so restore writes only the flagged ones
+	// instead of reading and rewriting the whole frame.
+	bool any_bg = false;
+	for (const FrameDesc &d : L.frames)
+		any_bg = any_bg || d.has_bg;
+	if (L.maxiter && any_bg)
+		ws.work.ensure(L.total_px);
 	for (size_t f = 0; f < nf; ++f) {
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
 		L.frames[f].floors = L.maxiter ? ws.floors.p + L.thr_base[f] : nullptr;
 		L.frames[f].rowcand = L.maxiter ? ws.rowmarks.p + L.row_off[f] : nullptr;
 		L.frames[f].rowchg = L.maxiter ? ws.rowmarks.p + L.row_words + L.row_off[f] : nullptr;
+		L.frames[f].out = L.frames[f].clean;
+		if (L.maxiter && L.frames[f].has_bg)
+			L.frames[f].clean = ws.work.p + L.offsets[f];
 	}
 	// Every descriptor array goes through one pinned staging buffer.  The
 	// previous call using this workspace synchronised before returning, so
@@ -865,32 +879,31 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 // (faster for error-map frames than any specialisation that was timed).
 static void launch_prepare(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s)
 {
-	bool model = true, bulk = true, rowmin = false;
+	bool model = true, bulk = true, rowmin = false, out = false;
 	for (const FrameDesc &fd : L.frames) {
 		const int kind = prep_kind(fd);
 		model = model && kind == PREP_MODEL;
 		bulk = bulk && prep_bulk_ok(fd);
 		rowmin = rowmin || kind == PREP_MODEL || kind == PREP_MODEL_MAPS;
+		out = out || (fd.out && fd.out != fd.clean);
 	}
 	const int nrows = (int)L.rows.size();
+	// Each variant is compiled for what the batch has (row minima, separate
+	// outputs): the kernels are issue-bound, and an unused branch costs.
 	if (bulk) {
 		const int need = (nrows + PB_WARPS - 1) / PB_WARPS, cap = di.sms * PB_BLOCKS;
 		const int grid = need < cap ? need : cap;
-		if (rowmin)
-			prepare_bulk_kernel<true><<<grid, 32 * PB_WARPS, PB_SMEM, s>>>(ws.frames.p, ws.state.p,
-				ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
-		else
-			prepare_bulk_kernel<false><<<grid, 32 * PB_WARPS, PB_SMEM, s>>>(ws.frames.p, ws.state.p,
-				ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
+		auto k = rowmin ? (out ? prepare_bulk_kernel<true, true> : prepare_bulk_kernel<true, false>)
+				: (out ? prepare_bulk_kernel<false, true> : prepare_bulk_kernel<false, false>);
+		k<<<grid, 32 * PB_WARPS, PB_SMEM, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows, ws.ctl.p,
+			ws.cands.p);
 		return;
 	}
 	const int grid = grid_for_rows(di, nrows, L.tune.row_blocks_per_sm);
-	if (model)
-		prepare_kernel<PREP_MODEL, 2 * ROW_UNROLL><<<grid, 256, 0, s>>>(ws.frames.p, ws.state.p,
-			ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
-	else
-		prepare_kernel<PREP_ANY><<<grid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows,
-			ws.ctl.p, ws.cands.p);
+	auto k = model ? (out ? prepare_kernel<PREP_MODEL, 2 * ROW_UNROLL, true>
+			       : prepare_kernel<PREP_MODEL, 2 * ROW_UNROLL, false>)
+		       : (out ? prepare_kernel<PREP_ANY, ROW_UNROLL, true> : prepare_kernel<PREP_ANY, ROW_UNROLL, false>);
+	k<<<grid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.rows.p, nrows, ws.ctl.p, ws.cands.p);
 }
 
 static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s,
@@ -1710,6 +1723,9 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 			L.frames[f].floors = p->L.frames[f].floors;
 			L.frames[f].rowcand = p->L.frames[f].rowcand;
 			L.frames[f].rowchg = p->L.frames[f].rowchg;
+			L.frames[f].out = L.frames[f].clean; // the new output buffer
+			if (p->L.frames[f].out != p->L.frames[f].clean) // working pixels in the workspace
+				L.frames[f].clean = p->L.frames[f].clean;
 		}
 		p->ims.assign(ims, ims + nf);
 		p->L.frames = L.frames;

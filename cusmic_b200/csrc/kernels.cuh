@@ -154,7 +154,7 @@ CB_HD int prep_kind(const FrameDesc &fd)
 // mask, BGMAP = background map.  Descriptor fields are held in registers (the
 // stores below go through pointers the compiler cannot prove distinct from
 // them).
-template <bool MASK, bool BGMAP, bool ROWMIN, int U = ROW_UNROLL>
+template <bool MASK, bool BGMAP, bool ROWMIN, int U = ROW_UNROLL, bool OUT = false>
 __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st, int f, int y,
 	Control *ctl, uint2 *holes)
 {
@@ -166,6 +166,10 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 	const uint8_t *__restrict__ mask = MASK && fd.mask ? fd.mask + rowpix : nullptr;
 	const double *__restrict__ bgmap = BGMAP && fd.bg_map ? fd.bg_map + rowpix : nullptr;
 	double *__restrict__ clean = fd.clean + rowpix;
+	// A separate output buffer (a frame with a background): its pixels now,
+	// (x + bg) - bg as the reference's restore computes them, the input at a
+	// hole; restore writes only the flagged ones.
+	double *__restrict__ out = OUT && fd.out && fd.out != fd.clean ? fd.out + rowpix : nullptr;
 	const double bgv = fd.bg;
 	const bool has_bg = fd.has_bg;
 	uint32_t *hole_plane = plane_ptr(fd, P_HOLE) + roww, *excl_plane = plane_ptr(fd, P_EXCL) + roww;
@@ -212,6 +216,8 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 					if (has_bg)
 						c += 1 * bg[u];
 					clean[x] = c;
+					if (out)
+						out[x] = hole ? d[u] : c + -1 * bg[u];
 					donor = ok && isfinite(c);
 				}
 				const uint32_t hw = __ballot_sync(0xffffffffu, hole);
@@ -266,7 +272,8 @@ __device__ __forceinline__ void prepare_row(const FrameDesc &fd, FrameState &st,
 // holes are appended to that list (count in ctl->n_holes) for the hole fill.
 // KIND: the frame kind every row has (PREP_ANY: decided per row); UL: the
 // unroll of the kinds without maps.
-template <int KIND = PREP_ANY, int UL = ROW_UNROLL>
+// OUT: some frame of the batch has a separate output buffer.
+template <int KIND = PREP_ANY, int UL = ROW_UNROLL, bool OUT = false>
 __global__ void __launch_bounds__(256, 4)
 prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
 	int nrows, Control *ctl = nullptr, uint2 *holes = nullptr)
@@ -278,19 +285,19 @@ prepare_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const in
 		FrameState &st = state[item.x];
 		switch (KIND == PREP_ANY ? prep_kind(fd) : KIND) {
 		case PREP_MODEL:
-			prepare_row<false, false, true, UL>(fd, st, item.x, item.y, ctl, holes);
+			prepare_row<false, false, true, UL, OUT>(fd, st, item.x, item.y, ctl, holes);
 			break;
 		case PREP_MODEL_MAPS:
-			prepare_row<true, true, true>(fd, st, item.x, item.y, ctl, holes);
+			prepare_row<true, true, true, ROW_UNROLL, OUT>(fd, st, item.x, item.y, ctl, holes);
 			break;
 		case PREP_MASK:
-			prepare_row<true, false, false, UL>(fd, st, item.x, item.y, ctl, holes);
+			prepare_row<true, false, false, UL, OUT>(fd, st, item.x, item.y, ctl, holes);
 			break;
 		case PREP_PLAIN:
-			prepare_row<false, false, false, UL>(fd, st, item.x, item.y, ctl, holes);
+			prepare_row<false, false, false, UL, OUT>(fd, st, item.x, item.y, ctl, holes);
 			break;
 		default:
-			prepare_row<true, true, false>(fd, st, item.x, item.y, ctl, holes);
+			prepare_row<true, true, false, ROW_UNROLL, OUT>(fd, st, item.x, item.y, ctl, holes);
 		}
 	}
 }
@@ -766,9 +773,13 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 		uint8_t *mask_out = fd.mask_out + rowpix;
 		const double bgv = fd.bg;
 		const bool has_bg = fd.has_bg;
-		if (!has_bg) { // warp-uniform
-			// clean already holds the output: only the mask and the restored
-			// non-finite inputs are written.  Groups of 32 bit words (1024
+		// A separate output buffer: prepare wrote every output pixel but the
+		// flagged ones (and restored the holes).
+		double *out = fd.out && fd.out != fd.clean ? fd.out + rowpix : nullptr;
+		if (!has_bg || out) { // warp-uniform
+			// clean (or out) already holds the output but for the flagged
+			// pixels of a separate output: only the mask, those pixels and
+			// the non-finite inputs are written.  Groups of 32 bit words (1024
 			// pixels), two groups' words loaded before either is used; a
 			// full group of an aligned row goes out as two contiguous
 			// 512-byte warp stores (lane j: the 16 pixels of half (j & 1) of
@@ -802,14 +813,27 @@ restore_kernel(const FrameDesc *__restrict__ frames, const int2 *__restrict__ ro
 							*reinterpret_cast<uint4 *>(mask_out + 32 * kb + 512 * q + 16 * lane) =
 								make_uint4(v[0], v[1], v[2], v[3]);
 						}
-					} else if (k < words) {
-						const int x0 = 32 * k, n = min(32, w - x0);
-						for (int i = 0; i < n; ++i)
-							mask_out[x0 + i] = (cw[g] >> i) & 1u;
+					} else {
+						// Unaligned rows: the group's words one after
+						// another, a lane per pixel (coalesced byte stores).
+						const int nk = min(32, words - kb);
+						for (int j = 0; j < nk; ++j) {
+							const uint32_t word = __shfl_sync(0xffffffffu, cw[g], j);
+							const int x = 32 * (kb + j) + lane;
+							if (x < w)
+								mask_out[x] = (word >> lane) & 1u;
+						}
 					}
-					for (uint32_t hb = hw[g]; hb; hb &= hb - 1) {
-						const int x = 32 * k + __ffs(hb) - 1;
-						clean[x] = data[x];
+					if (out) {
+						for (uint32_t fb = cw[g]; fb; fb &= fb - 1) {
+							const int x = 32 * k + __ffs(fb) - 1;
+							out[x] = clean[x] + -1 * (bgmap ? bgmap[x] : bgv);
+						}
+					} else {
+						for (uint32_t hb = hw[g]; hb; hb &= hb - 1) {
+							const int x = 32 * k + __ffs(hb) - 1;
+							clean[x] = data[x];
+						}
 					}
 				}
 			}

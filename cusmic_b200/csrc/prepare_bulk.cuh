@@ -88,7 +88,8 @@ __device__ __forceinline__ void seg_issue(PrepStage &S, int b, const SegCursor &
 }
 
 // ROWMIN: some frames are noise-model frames, whose row minima are written.
-template <bool ROWMIN>
+// OUT: some frame has a separate output buffer (a background).
+template <bool ROWMIN, bool OUT = false>
 __global__ void __launch_bounds__(32 * PB_WARPS, PB_BLOCKS)
 prepare_bulk_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int2 *__restrict__ rows,
 	int nrows, Control *ctl, uint2 *holes)
@@ -140,6 +141,8 @@ prepare_bulk_kernel(const FrameDesc *__restrict__ frames, FrameState *state, con
 		const bool rowmin = ROWMIN && fd.floors && !fd.error; // noise-model row minima
 		const double bgv = fd.bg;
 		double *__restrict__ clean = fd.clean + rowpix + x0;
+		// A separate output buffer (a frame with a background): as prepare_row.
+		double *__restrict__ out = OUT && fd.out && fd.out != fd.clean ? fd.out + rowpix + x0 : nullptr;
 		uint32_t my_h = 0, my_e = 0, my_d = 0, my_m = 0xffffffffu;
 #pragma unroll 4
 		for (int c = 0; c < PB_SEG / 32; ++c) {
@@ -158,6 +161,8 @@ prepare_bulk_kernel(const FrameDesc *__restrict__ frames, FrameState *state, con
 				if (has_bg)
 					v += 1 * bgv;
 				clean[xr] = v;
+				if (out)
+					out[xr] = hole ? d : v + -1 * bgv;
 				donor = ok_px && isfinite(v);
 			}
 			const uint32_t hw = __ballot_sync(0xffffffffu, hole);
