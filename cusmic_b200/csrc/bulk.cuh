@@ -36,16 +36,18 @@
 //    classes into the HIGH / LOW planes that incremental passes update.  The
 //    candidate kernels recompute every value they threshold exactly.
 //
-// sig_bulk_kernel is warp-specialised.  One producer warp copies clean row
+// sig_bulk_kernel is warp-specialised.  One producer thread copies clean row
 // segments (BK_COLS columns plus halo columns) into a ring of BK_SLOTS rows in
-// shared memory: lane 0 issues one `cp.async.bulk` for the 16-byte aligned
-// body of a row, lane 1 copies up to four single elements with 8-byte
-// `cp.async` (an unaligned first or last element, the border columns -1 and
-// w), so rows of any width and alignment stream the same way.  A row whose
-// aligned body starts on an odd cell is stored one cell to the right (its
-// shift).  Each ring row has a "full" mbarrier (lane 0's transaction bytes
-// plus lane 1's cp.async arrive) and an "empty" mbarrier on which each of the
-// four consumer warps arrives when it is done with the row.  (The S1, S2 and
+// shared memory: one `cp.async.bulk` for the 16-byte aligned body of a row
+// and up to four single elements with 8-byte `cp.async` (an unaligned first
+// or last element, the border columns -1 and w), so rows of any width and
+// alignment stream the same way.  A row whose aligned body starts on an odd
+// cell is stored one cell to the right (its shift).  Each ring row has a
+// "full" mbarrier (the body's transaction bytes plus the producer's cp.async
+// arrive) and an "empty" mbarrier on which each of the four consumer warps
+// arrives when it is done with the row.  The producer computes the copies of
+// an item's rows once per item (they differ by row offsets only), so its
+// per-row work is a wait on the row's empty barrier and the issue.  (The S1, S2 and
 // CAND planes were zeroed by the call's prologue memset.)  A block takes items
 // of BK_COLS x BK_ROWS pixels from a ticket counter (items of frames that
 // stopped are skipped there) and the ring runs straight through from one item
@@ -412,50 +414,78 @@ __device__ __forceinline__ unsigned hi_word(double v)
 	return (unsigned)__double2hiint(v);
 }
 
-// Producer warp of sig_bulk_kernel; g counts the ring rows issued.  Returns
-// false after a fault.
+// The copies of an in-frame row `by` elements (a whole number of row pairs)
+// away from the row b describes: only the element offsets into clean change
+// (-1, a zero, stays).
+__device__ __forceinline__ BulkRow shift_row(BulkRow b, long long by)
+{
+	b.src += by;
+	if (b.hsrc >= 0)
+		b.hsrc += by;
+	if (b.tsrc >= 0)
+		b.tsrc += by;
+	if (b.lsrc >= 0)
+		b.lsrc += by;
+	if (b.rsrc >= 0)
+		b.rsrc += by;
+	return b;
+}
+
+// Issue the copies of one ring row (one thread: the bulk copy completes on
+// the row's full barrier by its transaction bytes, the single-element copies
+// by the thread's cp.async arrival).
+__device__ __forceinline__ void bulk_issue(BulkRing &R, int slot, const BulkRow &b, const double *clean)
+{
+	double *row = R.c[slot];
+	R.shift[slot] = b.shift;
+	mbar_expect_tx(&R.full[slot], b.bytes);
+	if (b.n)
+		bulk_copy(row + b.cell, b.src < 0 ? bulk_zero_row : clean + b.src, 8u * b.n, &R.full[slot]);
+	if (b.hsrc != NO_COPY)
+		cp_async8(row + b.hcell, clean + b.hsrc);
+	if (b.tsrc != NO_COPY)
+		cp_async8(row + b.tcell, clean + b.tsrc);
+	if (b.lsrc != NO_COPY)
+		cp_async8(row + b.lcell, b.lsrc < 0 ? bulk_zero_row : clean + b.lsrc);
+	if (b.rsrc != NO_COPY)
+		cp_async8(row + b.rcell, b.rsrc < 0 ? bulk_zero_row : clean + b.rsrc);
+	mbar_arrive_cp_async(&R.full[slot]);
+}
+
+// Producer of sig_bulk_kernel: one thread (lane 0 of the producer warp); g
+// counts the ring rows issued.  Returns false after a fault.  The copies of
+// an item's in-frame rows differ only by their row offsets, in two classes
+// by row parity (the 16-byte phase of a row start alternates when w is odd),
+// so they are computed once per item (kept in `base`, shared memory); rows
+// outside the frame (border-mapped or zero) are computed on their own.
 __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__restrict__ frames,
 	const FrameState *__restrict__ state, const int4 *__restrict__ items, int nitems, int lm,
-	Control *ctl, int &g)
+	Control *ctl, int &g, BulkRow (&base)[2])
 {
-	const int lane = threadIdx.x & 31;
-	int next = 0;
-	bool ok = true;
-	if (lane == 0)
-		next = atomicAdd(&ctl->ticket, 1);
+	int next = atomicAdd(&ctl->ticket, 1);
 	for (;;) {
-		// Next active item (lane 0 decides, the warp follows).
+		// Next active item.
 		int t = -1;
-		if (lane == 0) {
-			while (next < nitems) {
-				const int cand = next;
-				next = atomicAdd(&ctl->ticket, 1);
-				const int4 it = items[cand];
-				if (!state[it.x].active)
-					continue;
-				if ((uintptr_t)frames[it.x].clean & 7) // the host rejects such buffers
-					ok = false;
-				else
-					t = cand;
-				break;
-			}
+		while (next < nitems) {
+			const int cand = next;
+			next = atomicAdd(&ctl->ticket, 1);
+			const int4 it = items[cand];
+			if (!state[it.x].active)
+				continue;
+			if ((uintptr_t)frames[it.x].clean & 7) // the host rejects such buffers
+				return false;
+			t = cand;
+			break;
 		}
-		if (!__shfl_sync(0xffffffffu, ok, 0))
-			return false;
-		t = __shfl_sync(0xffffffffu, t, 0);
 		if (t < 0) { // end of the list: an end marker in the next ring row
 			const int slot = g & (BK_SLOTS - 1);
-			if (lane == 0) {
-				ok = g < BK_SLOTS || mbar_wait(&R.empty[slot], ((g / BK_SLOTS) - 1) & 1, &R.abort);
-				if (ok) {
-					R.meta[slot] = make_int2(-1, 0);
-					mbar_arrive(&R.full[slot]);
-					mbar_arrive(&R.full[slot]);
-				}
-			}
-			ok = __shfl_sync(0xffffffffu, ok, 0);
-			g += ok;
-			return ok;
+			if (g >= BK_SLOTS && !mbar_wait(&R.empty[slot], ((g / BK_SLOTS) - 1) & 1, &R.abort))
+				return false;
+			R.meta[slot] = make_int2(-1, 0);
+			mbar_arrive(&R.full[slot]);
+			mbar_arrive(&R.full[slot]);
+			++g;
+			return true;
 		}
 		const int4 it = items[t];
 		const FrameDesc &fd = frames[it.x];
@@ -463,34 +493,19 @@ __device__ __forceinline__ bool bulk_producer(BulkRing &R, const FrameDesc *__re
 		const int y1 = it.w; // items never cross a 32-row floor block
 		const double *clean = fd.clean;
 		const int mis = (int)(((uintptr_t)clean >> 3) & 1);
+		const int ra = y0 - 1 < 0 ? 0 : y0 - 1; // first in-frame row of the item
+		base[0] = bulk_row(w, h, lm, mis, x0, ra);
+		base[1] = bulk_row(w, h, lm, mis, x0, ra + 1 < h ? ra + 1 : ra);
 		for (int r = y0 - 1; r <= y1; ++r) {
 			const int slot = g & (BK_SLOTS - 1);
-			if (lane == 0)
-				ok = g < BK_SLOTS || mbar_wait(&R.empty[slot], ((g / BK_SLOTS) - 1) & 1, &R.abort);
-			if (!__shfl_sync(0xffffffffu, ok, 0))
+			const int d = r - ra;
+			const BulkRow b = r < 0 || r >= h ? bulk_row(w, h, lm, mis, x0, r)
+				: shift_row(base[d & 1], (long long)(d & ~1) * w);
+			if (g >= BK_SLOTS && !mbar_wait(&R.empty[slot], ((g / BK_SLOTS) - 1) & 1, &R.abort))
 				return false;
-			__syncwarp();
-			const BulkRow b = bulk_row(w, h, lm, mis, x0, r);
-			double *row = R.c[slot];
-			if (lane == 0) {
-				if (r == y0 - 1)
-					R.meta[slot] = make_int2(t, y1);
-				R.shift[slot] = b.shift;
-				mbar_expect_tx(&R.full[slot], b.bytes);
-				if (b.n)
-					bulk_copy(row + b.cell, b.src < 0 ? bulk_zero_row : clean + b.src, 8u * b.n,
-						&R.full[slot]);
-			} else if (lane == 1) {
-				if (b.hsrc != NO_COPY)
-					cp_async8(row + b.hcell, clean + b.hsrc);
-				if (b.tsrc != NO_COPY)
-					cp_async8(row + b.tcell, clean + b.tsrc);
-				if (b.lsrc != NO_COPY)
-					cp_async8(row + b.lcell, b.lsrc < 0 ? bulk_zero_row : clean + b.lsrc);
-				if (b.rsrc != NO_COPY)
-					cp_async8(row + b.rcell, b.rsrc < 0 ? bulk_zero_row : clean + b.rsrc);
-				mbar_arrive_cp_async(&R.full[slot]);
-			}
+			if (r == y0 - 1)
+				R.meta[slot] = make_int2(t, y1);
+			bulk_issue(R, slot, b, clean);
 			++g;
 		}
 	}
@@ -671,10 +686,11 @@ sig_bulk_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 	int *pre_counts)
 {
 	__shared__ BulkRing R;
+	__shared__ BulkRow base[2]; // the producer's row copies of the current item
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	if (tid == 0) {
 		for (int i = 0; i < BK_SLOTS; ++i) {
-			mbar_init(&R.full[i], 2); // producer lanes 0 (bytes) and 1 (cp.async)
+			mbar_init(&R.full[i], 2); // the producer's transaction bytes and cp.async arrive
 			mbar_init(&R.empty[i], BK_CWARPS);
 		}
 		mbar_init(&R.poison, 1);
@@ -685,7 +701,8 @@ sig_bulk_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 	bool ok;
 	int issued = 0; // ring rows issued (producer warp)
 	if (warp == BK_CWARPS)
-		ok = bulk_producer(R, frames, state, items, nitems, lap_mode(prm.mode), ctl, issued);
+		ok = lane || bulk_producer(R, frames, state, items, nitems, lap_mode(prm.mode), ctl, issued,
+			base);
 	else if (warp == 0 && blockIdx.x == 0 && ctl->poison_wait[1] > 0)
 		ok = __all_sync(0xffffffffu, poisoned_wait(&R.poison, &R.abort, ctl->poison_wait[1]));
 	else

@@ -368,6 +368,7 @@ struct Layout {
 	std::vector<long long> row_off; // first row of each frame in the row marks
 	long long row_words = 0;        // row marks of all frames, padded to 4
 	std::vector<int4> bulk;   // sig_bulk_kernel items {frame, x0, y0, first threshold of the frame}
+	std::vector<int4> grow;   // grow_kernel items {frame, y0, first word, y1}
 	std::vector<FloorJob> jobs; // floor blocks of each distinct error map and noise-model frame
 	std::vector<long long> thr_base; // per frame: first floor of its blocks
 	long long nthr = 0;
@@ -421,6 +422,7 @@ struct Workspace {
 	DevBuf<double> work;    // working pixels of the frames with a background
 	DevBuf<uint2> cands;
 	DevBuf<int4> bulk;
+	DevBuf<int4> grow;
 	DevBuf<FloorJob> jobs;
 	DevBuf<BlockFloor> floors;
 	DevBuf<PreCand> pre;
@@ -644,6 +646,9 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 		for (int ty = 0; ty < d.h; ty += rows_per_item)
 			for (int tx = 0; tx < d.w; tx += BK_COLS)
 				L.bulk.push_back(make_int4((int)f, tx, ty, std::min(ty + rows_per_item, d.h)));
+		for (int ty = 0; ty < d.h; ty += GROW_ROWS)
+			for (int k0 = 0; k0 < d.words; k0 += 32)
+				L.grow.push_back(make_int4((int)f, ty, k0, std::min(ty + GROW_ROWS, d.h)));
 	}
 	L.total_px = px;
 	L.row_words = (L.row_words + 3) & ~3ll;
@@ -681,6 +686,7 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s, bool mapped = false
 	ws.frames.ensure(nf);
 	ws.state.ensure(nf);
 	ws.bulk.ensure(L.bulk.size() ? L.bulk.size() : 1);
+	ws.grow.ensure(L.grow.size() ? L.grow.size() : 1);
 	ws.jobs.ensure(L.jobs.size() ? L.jobs.size() : 1);
 	ws.floors.ensure(L.nthr ? (size_t)L.nthr : 1);
 	ws.rows.ensure(L.rows.size());
@@ -729,6 +735,7 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s, bool mapped = false
 		{ws.frames.p, L.frames.data(), nf * sizeof(FrameDesc)},
 		{ws.rows.p, L.rows.data(), L.rows.size() * sizeof(int2)},
 		{ws.bulk.p, L.bulk.data(), L.bulk.size() * sizeof(int4)},
+		{ws.grow.p, L.grow.data(), L.grow.size() * sizeof(int4)},
 		{ws.jobs.p, L.jobs.data(), L.jobs.size() * sizeof(FloorJob)},
 		{ws.offsets.p, L.offsets.data(), nf * sizeof(long long)},
 	};
@@ -858,16 +865,19 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 		candidate_low_kernel<PATH_MODEL><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
 			ws.ctl.p, !incremental);
 	mark(rec, K_LOW);
-	// An incremental pass grows on its dirty rows only.
-	grow_update_kernel<<<grid_for_rows(di, nrows, rowb), 256, 0, s>>>(ws.frames.p, ws.state.p,
-		incremental ? ws.dirty.p : ws.rows.p, nrows, incremental ? &ws.ctl.p->n_dirty : nullptr,
-		ws.targets.p, ws.ctl.p);
+	// Growth visits the items holding marked rows.
+	{
+		const int ng = (int)L.grow.size(), need = (ng + 7) / 8, gcap = di.sms * rowb;
+		grow_kernel<<<need < gcap ? need : gcap, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.grow.p, ng,
+			ws.targets.p, ws.ctl.p);
+	}
 	mark(rec, K_GROW);
 	control_kernel<<<1, 1024, 0, s>>>(ws.state.p, nf, ws.ctl.p, gl.handle, gl.use ? 1 : 0);
 	mark(rec, K_CONTROL);
 	const int tb = di.sms * 4;
 	replace_select_kernel<<<tb, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
-		&ws.ctl.p->n_targets, ws.radius.p, ws.ctl.p, ws.sel.p);
+		&ws.ctl.p->n_targets, ws.radius.p, ws.ctl.p, ws.sel.p,
+		reinterpret_cast<uint4 *>(ws.rowmarks.p + L.row_words), L.row_words / 4);
 	replace_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
 		&ws.ctl.p->n_targets, ws.sel.p, &ws.ctl.p->n_sel, ws.radius.p);
 	mark(rec, K_REPLACE);
@@ -2071,6 +2081,8 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 		init_kernel<<<1, 256, 0, s>>>(state, 1, ctl, o->maxiter,
 			(unsigned long long)im->width * im->height);
 		const int row_blocks = (h + 7) / 8 < nd.sms * 8 ? (h + 7) / 8 : nd.sms * 8;
+		const int grow_items = (h + GROW_ROWS - 1) / GROW_ROWS * ((fd.words + 31) / 32);
+		const int grow_blocks = (grow_items + 7) / 8 < nd.sms * 8 ? (grow_items + 7) / 8 : nd.sms * 8;
 		if (!o->maxiter) {
 			copy_kernel<<<row_blocks, 256, 0, s>>>(frames, rows, h);
 		} else {
@@ -2094,7 +2106,7 @@ extern "C" int remove_cosmics_device_noalloc(const cusmic_image *im, const cusmi
 					seeds, 1);
 				seed_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, seeds, prm, ctl, 1);
 				candidate_low_kernel<PATH_ANY><<<nd.sms * 8, 256, 0, s>>>(frames, cands, prm, ctl, 1);
-				grow_update_kernel<<<row_blocks, 256, 0, s>>>(frames, state, rows, h, nullptr, targets,
+				grow_kernel<<<grow_blocks, 256, 0, s>>>(frames, state, nullptr, grow_items, targets,
 					ctl);
 				control_kernel<<<1, 1024, 0, s>>>(state, 1, ctl, 0, 0);
 				replace_kernel<<<nd.sms * 8, 256, 0, s>>>(frames, state, targets, &ctl->n_targets, nullptr,

@@ -32,9 +32,10 @@
 // The row kernel dilates CHG with bit windows (one warp per row, a lane per
 // bit word), so every pixel is visited once without atomics.  The candidate
 // and seed kernels then run on those lists exactly as in a full pass,
-// setting or clearing each bit they evaluate, and growth visits the dirty
-// rows (fresh pixels lie within 6 of D), clearing their CHG bits and row
-// marks before the replacement writes the next D.  What stays exact: S1 and CAND
+// setting or clearing each bit they evaluate, and growth visits the items
+// holding dirty rows (fresh pixels lie within 6 of D), clearing their CHG
+// bits (replace_select_kernel clears the CHG row marks) before the
+// replacement writes the next D.  What stays exact: S1 and CAND
 // everywhere, S2 of every HIGH pixel and of every LOW pixel with a CAND pixel
 // within 2 (the only S2 bits growth reads): a LOW pixel whose CAND
 // neighbourhood changed is within 6 of D.  Outside HIGH sig <= cr_threshold,
@@ -108,7 +109,8 @@ __device__ __forceinline__ bool rows_changed(const FrameDesc &fd, int y, int r, 
 }
 
 // The rows of active frames with a changed pixel within six rows, appended
-// to `out` (count in ctl->n_dirty) and marked for growth.  A thread per row.
+// to `out` (count in ctl->n_dirty); every row of an active frame gets its
+// growth mark (set on those rows, cleared on the others).  A thread per row.
 // The same threads first zero `clear` (n16 16-byte words: the FRESH plane,
 // which this pass's growth writes on the rows it visits and the previous
 // pass's replacement has read).
@@ -131,8 +133,7 @@ dirty_rows_kernel(const FrameDesc *__restrict__ frames, const FrameState *__rest
 			if (state[item.x].active) {
 				const FrameDesc &fd = frames[item.x];
 				keep = rows_changed(fd, item.y, 6, wrap);
-				if (keep)
-					fd.rowcand[item.y] = 1u;
+				fd.rowcand[item.y] = keep; // replaces the last pass's marks
 			}
 		}
 		const unsigned b = __ballot_sync(0xffffffffu, keep);

@@ -321,88 +321,136 @@ __device__ __forceinline__ unsigned long long dilate_row(unsigned long long e)
 	return e | (e << 1) | (e >> 1);
 }
 
+// Rows of a growth item (grow_kernel).
+constexpr int GROW_ROWS = 16;
+
+// 36-bit window of a bit-plane row (bit_window) for a lane whose word is past
+// the row: zero.
+__device__ __forceinline__ unsigned long long lane_window(const uint32_t *plane, int words, int h,
+	int y, int k)
+{
+	return k < words ? bit_window(plane, words, h, y, k) : 0ull;
+}
+
 // Reference src/filters.cuh:177-193 twice (src/cleaner.cuh:123-125) and
 // src/cleaner.cuh:22-37: grown = dilate3x3(dilate3x3(cand) & S1) & S2 on bit
-// planes, fresh = grown & ~crmask, crmask |= grown, the FRESH plane, the
-// per-frame facts (any fresh pixel; the count of static donors left, which
-// the reference recounts in accumulate), and fresh pixels appended to the
-// target list.  The row list holds nrows rows, or *dev_nrows when that is
-// not null.  With row marks (fd.rowcand) an unmarked row is skipped: nothing
-// can grow there, and its FRESH words were zeroed before the pass.  A full
-// pass marks the rows within two of a CAND pixel (two 3 x 3 dilations); an
-// incremental pass lists the rows within six of a pixel whose value the last
-// replacement changed, and marks them.  A visited row's CHG bits and mark are
-// cleared (every row with a CHG bit is visited).
-__global__ void __launch_bounds__(256, 5)
-grow_update_kernel(const FrameDesc *__restrict__ frames, FrameState *state,
-	const int2 *__restrict__ rows, int nrows, const int *dev_nrows, uint2 *targets, Control *ctl)
+// planes (clipped to the frame), fresh = grown & ~crmask, crmask |= grown,
+// the FRESH plane, the per-frame facts (any fresh pixel; the count of static
+// donors left, which the reference recounts in accumulate), and fresh pixels
+// appended to the target list.
+//
+// One warp per item of GROW_ROWS rows x 32 bit words (a lane per word), from
+// `items` {frame, first row, first word, end row}, or with items null from
+// frame 0 in row-major item order.  The warp sweeps down its rows keeping the
+// horizontal dilations of the CAND rows y .. y + 1 and of the S1-masked rows
+// y - 1 .. y in registers, so each row step reads one CAND window, an S1
+// window only where a dilated CAND pixel is near, S2 and CRMASK only where
+// something can grow, and DONOR only where pixels are flagged; the item
+// appends its fresh pixels with one atomic.  (Issuing the loads of four rows
+// together, unconditionally, measured slower.)
+//
+// With row marks (fd.rowcand) an item none of whose rows is marked is
+// skipped: a full pass marks the rows within two of a CAND pixel (nothing
+// grows elsewhere), an incremental pass the rows within six of a pixel whose
+// value the last replacement changed (elsewhere grown repeats the last pass
+// and is already in the mask).  A visited item computes all its rows (an
+// unmarked row adds nothing) and clears the CHG bits of its rows with a CHG
+// mark (every such row is marked; replace_select_kernel then clears the
+// marks).  FRESH is written on every visited row (the pass starts with it
+// zeroed where it skips).
+__global__ void __launch_bounds__(256)
+grow_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int4 *__restrict__ items,
+	int nitems, uint2 *targets, Control *ctl)
 {
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-	if (dev_nrows)
-		nrows = *dev_nrows;
-	for (int r = gw; r < nrows; r += nw) {
-		const int2 item = rows[r];
-		if (!state[item.x].active)
-			continue; // warp-uniform
-		const FrameDesc &fd = frames[item.x];
-		const int w = fd.w, h = fd.h, y = item.y, words = fd.words;
-		if (fd.rowcand && !fd.rowcand[y])
-			continue; // warp-uniform: no pixel of the row can be flagged this pass
-		if (fd.rowchg && fd.rowchg[y]) {
-			// The pass has read the row's CHG bits: clear them for the
-			// replacement that follows.
-			for (int k = lane; k < words; k += 32)
-				plane_ptr(fd, P_CHG)[(long long)y * words + k] = 0u;
-			if (lane == 0)
-				fd.rowchg[y] = 0u;
+	for (int i = gw; i < nitems; i += nw) {
+		int4 it;
+		if (items) {
+			it = items[i];
+		} else {
+			const int strips = (frames[0].words + 31) / 32, y0 = (i / strips) * GROW_ROWS;
+			it = make_int4(0, y0, (i % strips) * 32, min(y0 + GROW_ROWS, frames[0].h));
 		}
+		const int f = it.x;
+		if (!state[f].active)
+			continue; // warp-uniform
+		const FrameDesc &fd = frames[f];
+		const int w = fd.w, h = fd.h, words = fd.words, y0 = it.y, n = it.w - it.y, k = it.z + lane;
+		const bool row_lane = lane < n;
+		const unsigned visit = __ballot_sync(0xffffffffu,
+			row_lane && (!fd.rowcand || fd.rowcand[y0 + lane]));
+		if (!visit)
+			continue; // warp-uniform
+		const unsigned chg = fd.rowchg
+			? __ballot_sync(0xffffffffu, row_lane && fd.rowchg[y0 + lane]) : 0u;
 		const uint32_t *cand = plane_ptr(fd, P_CAND), *s1 = plane_ptr(fd, P_S1);
 		const uint32_t *s2 = plane_ptr(fd, P_S2), *donor = plane_ptr(fd, P_DONOR);
-		uint32_t *crm = plane_ptr(fd, P_CRMASK);
-		uint32_t todo = 0;
-		int lost = 0; // static donors this row added to the mask
-		for (int k0 = 0; k0 < words; k0 += 32) {
-			const int k = k0 + lane;
-			uint32_t fresh = 0;
+		uint32_t *crm = plane_ptr(fd, P_CRMASK), *fr = plane_ptr(fd, P_FRESH);
+		uint32_t *cg = plane_ptr(fd, P_CHG);
+		// Dilated CAND rows y0 - 2 .. y0 + 1, then the dilated S1-masked rows
+		// y0 - 1 and y0 (h0, h1); c0, c1: dilated CAND rows y and y + 1.
+		unsigned long long c0, c1, h0, h1;
+		{
+			const unsigned long long d0 = dilate_row(lane_window(cand, words, h, y0 - 2, k));
+			const unsigned long long d1 = dilate_row(lane_window(cand, words, h, y0 - 1, k));
+			c0 = dilate_row(lane_window(cand, words, h, y0, k));
+			c1 = dilate_row(lane_window(cand, words, h, y0 + 1, k));
+			const unsigned long long a = d0 | d1 | c0, b = d1 | c0 | c1;
+			h0 = a ? dilate_row(a & lane_window(s1, words, h, y0 - 1, k)) : 0ull;
+			h1 = b ? dilate_row(b & lane_window(s1, words, h, y0, k)) : 0ull;
+		}
+		int cnt = 0, lost = 0;
+		unsigned rows_fresh = 0; // bit j: this lane flagged pixels in row y0 + j
+#pragma unroll 4
+		for (int j = 0; j < n; ++j) {
+			const int y = y0 + j;
+			const unsigned long long c2 = dilate_row(lane_window(cand, words, h, y + 2, k));
+			const unsigned long long cc = c0 | c1 | c2;
+			const unsigned long long h2 = cc ? dilate_row(cc & lane_window(s1, words, h, y + 1, k)) : 0ull;
+			const uint32_t near = (uint32_t)((h0 | h1 | h2) >> 2); // bits 2..33: the word's pixels
 			if (k < words) {
-				unsigned long long c[5], g1[3];
-#pragma unroll
-				for (int d = 0; d < 5; ++d)
-					c[d] = dilate_row(bit_window(cand, words, h, y - 2 + d, k));
-#pragma unroll
-				for (int d = 0; d < 3; ++d)
-					g1[d] = bit_window(s1, words, h, y - 1 + d, k) & (c[d] | c[d + 1] | c[d + 2]);
-				unsigned long long g2 = ((unsigned long long)s2[(long long)y * words + k] << 2) &
-					(dilate_row(g1[0]) | dilate_row(g1[1]) | dilate_row(g1[2]));
-				const uint32_t grown = (uint32_t)(g2 >> 2);
 				const long long o = (long long)y * words + k;
-				const uint32_t old = crm[o];
-				fresh = grown & ~old;
-				const uint32_t now = old | grown;
-				if (fresh)
-					crm[o] = now;
-				plane_ptr(fd, P_FRESH)[o] = fresh;
-				todo |= fresh;
-				lost += __popc(fresh & donor[o]);
+				uint32_t fresh = 0;
+				if (near) {
+					const uint32_t grown = near & s2[o], old = crm[o];
+					fresh = grown & ~old;
+					if (fresh) {
+						crm[o] = old | fresh;
+						cnt += __popc(fresh);
+						lost += __popc(fresh & donor[o]);
+						rows_fresh |= 1u << j;
+					}
+				}
+				fr[o] = fresh;
+				if ((chg >> j) & 1u)
+					cg[o] = 0u;
 			}
-			if (__any_sync(0xffffffffu, fresh != 0)) {
-				unsigned long long slot = warp_append(&ctl->n_targets, __popc(fresh));
+			c0 = c1;
+			c1 = c2;
+			h0 = h1;
+			h1 = h2;
+		}
+		const bool any = __any_sync(0xffffffffu, cnt != 0);
+		if (any) {
+			unsigned long long slot = warp_append(&ctl->n_targets, cnt);
+			for (unsigned m = rows_fresh; m; m &= m - 1) {
+				const int y = y0 + __ffs(m) - 1;
+				uint32_t fresh = fr[(long long)y * words + k]; // this lane's own store
 				const unsigned base = (unsigned)((long long)y * w + 32 * k);
 				while (fresh) {
-					int b = __ffs(fresh) - 1;
+					const int b = __ffs(fresh) - 1;
 					fresh &= fresh - 1;
-					targets[slot++] = make_uint2((unsigned)item.x, base + b);
+					targets[slot++] = make_uint2((unsigned)f, base + b);
 				}
 			}
 		}
-		todo = __any_sync(0xffffffffu, todo != 0);
 		lost = __reduce_add_sync(0xffffffffu, (unsigned)lost);
 		if (lane == 0) {
-			if (todo)
-				set_flag(&state[item.x].todo);
+			if (any)
+				set_flag(&state[f].todo);
 			if (lost)
-				atomicAdd((unsigned long long *)&state[item.x].donors_left,
+				atomicAdd((unsigned long long *)&state[f].donors_left,
 					(unsigned long long)(-(long long)lost));
 		}
 	}
@@ -631,7 +679,9 @@ __device__ __forceinline__ bool fresh_in_window(const FrameDesc &fd, int x, int 
 
 // Which targets the replacement after a pass must visit, for frames whose
 // pass flagged new pixels: a lane per target; the indices of those to visit
-// are appended to `sel` (count in ctl->n_sel).
+// are appended to `sel` (count in ctl->n_sel).  The same threads first zero
+// `clear` (n16 16-byte words: the CHG row marks, which this pass has read
+// and the replacement that follows sets).
 //
 // radius keeps, per target, the window radius of its last replacement.  A
 // target whose last window (radius r <= KEEP_RADIUS_MAX) holds no pixel the
@@ -642,11 +692,13 @@ __device__ __forceinline__ bool fresh_in_window(const FrameDesc &fd, int x, int 
 __global__ void __launch_bounds__(256)
 replace_select_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const uint2 *__restrict__ list, const unsigned long long *count,
-	const uint8_t *__restrict__ radius, Control *ctl, unsigned *sel)
+	const uint8_t *__restrict__ radius, Control *ctl, unsigned *sel, uint4 *clear, long long n16)
 {
 	const int lane = threadIdx.x & 31;
 	const long long n = (long long)*count;
 	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += stride)
+		clear[i] = make_uint4(0u, 0u, 0u, 0u);
 	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
 	     base += stride) {
 		const long long e = base + lane;
@@ -908,7 +960,7 @@ struct WordCopy {
 };
 
 struct WordCopies {
-	WordCopy part[5];
+	WordCopy part[6];
 	int n;
 };
 
