@@ -597,6 +597,77 @@ __device__ double select_rank(const FrameDesc &fd, const uint32_t *don, const ui
 	return order_value(prefix);
 }
 
+// The donors of a window of 33 .. 32 S cells in key order, for the median:
+// lane l holds the keys of cells l + 32 s (all ones for a non-donor or a cell
+// past the window, which sort last), a bitonic network sorts the warp's 32 S
+// keys in unsigned order (the order select_rank's radix select ranks by),
+// and the keys of ranks (nd - 1) / 2 and nd / 2 come back as lo and hi.
+// Returns nd, the number of donors (0: lo and hi unset).  About 20 to 30
+// dependent exchange steps instead of select_rank's 64 warp reductions per
+// rank, so a replacement whose window grew past 5 x 5 no longer holds its
+// launch for tens of microseconds.
+template <int S>
+__device__ __noinline__ int sorted_window_median(const FrameDesc &fd, const uint32_t *don,
+	const uint32_t *crm, Window win, double &lo, double &hi)
+{
+	const int lane = threadIdx.x & 31;
+	const int ww = win.x1 - win.x0 + 1, area = ww * (win.y1 - win.y0 + 1);
+	unsigned long long k[S];
+	int nd = 0;
+#pragma unroll
+	for (int s = 0; s < S; ++s) {
+		const int pos = lane + 32 * s;
+		k[s] = ~0ull;
+		if (pos < area) {
+			const int x = win.x0 + pos % ww, y = win.y0 + pos / ww;
+			if (donor_at(don, crm, fd.words, x, y))
+				k[s] = order_key(fd.clean[(long long)y * fd.w + x]);
+		}
+		nd += __popc(__ballot_sync(0xffffffffu, k[s] != ~0ull));
+	}
+	if (!nd)
+		return 0;
+	// Element i = 32 s + lane; ascending where bit `size` of i is clear.
+#pragma unroll
+	for (int size = 2; size <= 32 * S; size <<= 1) {
+#pragma unroll
+		for (int j = size >> 1; j > 0; j >>= 1) {
+			if (j >= 32) { // partner in the same lane, slot s ^ (j / 32)
+#pragma unroll
+				for (int s = 0; s < S; ++s) {
+					const int t = s ^ (j >> 5);
+					if (t < s)
+						continue;
+					const bool asc = ((32 * s + lane) & size) == 0;
+					const unsigned long long a = k[s], b = k[t];
+					const bool swap = asc ? b < a : a < b;
+					k[s] = swap ? b : a;
+					k[t] = swap ? a : b;
+				}
+			} else { // partner lane ^ j, same slot
+#pragma unroll
+				for (int s = 0; s < S; ++s) {
+					const unsigned long long p = __shfl_xor_sync(0xffffffffu, k[s], j);
+					const bool keep_min = ((lane & j) == 0) == (((32 * s + lane) & size) == 0);
+					k[s] = keep_min ? (p < k[s] ? p : k[s]) : (k[s] < p ? p : k[s]);
+				}
+			}
+		}
+	}
+	const int rl = (nd - 1) / 2, rh = nd / 2;
+	unsigned long long vl = 0, vh = 0;
+#pragma unroll
+	for (int s = 0; s < S; ++s) { // register slots chosen by unrolled tests, not indexed
+		if (s == rl >> 5)
+			vl = k[s];
+		if (s == rh >> 5)
+			vh = k[s];
+	}
+	lo = order_value(__shfl_sync(0xffffffffu, vl, rl & 31));
+	hi = order_value(__shfl_sync(0xffffffffu, vh, rh & 31));
+	return nd;
+}
+
 // Reference src/replace.cuh:111-153 for one pixel, by the whole warp: the
 // median of the donors in the clipped (2r+1)^2 window, r = 2, 3, ... until a
 // donor exists; lane 0 writes it.  Returns r (0: the frame has no donor).
@@ -629,6 +700,14 @@ __device__ __forceinline__ int replace_one(const FrameDesc &fd, int x, int y, bo
 			v = bitonic32(v);
 			lo = __shfl_sync(0xffffffffu, v, (nd - 1) / 2);
 			hi = __shfl_sync(0xffffffffu, v, nd / 2);
+		} else if (area <= 64) {
+			nd = sorted_window_median<2>(fd, don, crm, win, lo, hi);
+			if (!nd)
+				continue;
+		} else if (area <= 128) {
+			nd = sorted_window_median<4>(fd, don, crm, win, lo, hi);
+			if (!nd)
+				continue;
 		} else {
 			int cnt = 0;
 			for (int pos = lane; pos < area; pos += 32)

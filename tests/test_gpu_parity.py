@@ -653,3 +653,32 @@ def test_prepare_unaligned_input(cuda, oracle):
     (clean, got_mask), = fr.outputs()
     np.testing.assert_array_equal(got_mask, want_mask)
     assert_bits_equal(clean, want_clean)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_large_replacement_windows(cuda, oracle, seed):
+    """Square blocks of holes (3 to 17 pixels across) and masked squares next
+    to cosmic rays, on a sky of few distinct values with signed zeros, so the
+    hole fill and the replacement use windows from 5 x 5 up past 16 x 16:
+    every median path (a warp sort of 25, the sorted keys of up to 64 and 128
+    cells, the radix select beyond) must pick the reference's ranks in key
+    order, -0 below +0."""
+    rng = np.random.default_rng(7100 + seed)
+    h, w = int(rng.integers(48, 96)), int(rng.integers(48, 96))
+    data = rng.choice(np.array([-0.0, 0.0, 1.0, -1.0, 2.0, 0.5]), size=(h, w))
+    mask = np.zeros((h, w), bool)
+    for size in (3, 5, 7, 9, 11, 13, 17):
+        y, x = int(rng.integers(0, h - size)), int(rng.integers(0, w - size))
+        data[y:y + size, x:x + size] = np.nan
+    for size in (6, 10, 14):
+        y, x = int(rng.integers(1, h - size - 1)), int(rng.integers(1, w - size - 1))
+        mask[y:y + size, x:x + size] = True
+        data[y + size // 2, x - 1] += 5000.0  # a ray at the block's edge grows into it
+        data[y + size // 2, x] += 3000.0
+    frame = dict(data=data, mask=mask, error=np.full((h, w), 0.3))
+    if seed % 2:
+        frame = dict(data=data + 3.0, mask=mask, gain=1.5, readnoise=0.5)
+    opts = dict(SETTINGS, maxiter=3, border=MODES[seed % len(MODES)])
+    if "gain" in frame:
+        opts.update(gain=1.5, readnoise=0.5)
+    check_against_oracle(oracle, [frame], opts)
