@@ -27,7 +27,8 @@ EXPORTS = (
 )
 TUNING_PATH = Path(__file__).with_name("tuning.json")
 KERNEL_KINDS = ("init", "prepare", "fill", "sigraw", "cand", "seed", "grow", "control",
-                "replace", "restore", "copy", "low", "classify", "floor", "reclass", "dirty")
+                "replace", "restore", "copy", "low", "classify", "floor", "reclass", "dirty",
+                "sigmap")
 
 
 class Image(ctypes.Structure):

@@ -106,6 +106,10 @@ struct FrameDesc {
 	BlockFloor *floors; // the frame's block floors, row-major by block (null: none)
 	uint32_t *rowcand;  // per row: nonzero when growth must visit the row this pass (null: all)
 	uint32_t *rowchg;   // per row: nonzero when the row has a CHG pixel (null: no tracking)
+	// Noise-model frames, first pass: sig_raw and the noise at every pixel
+	// within two of a HIGH pixel (region_sig_kernel), which the high-list
+	// candidates read instead of recomputing their windows (null: none).
+	double *sig_raw, *noise;
 	double gain, rn, bg;
 	long long plane;   // words per plane of this frame = h * words
 	long long pstride; // words from one plane to the next (planes of all frames of a
@@ -142,6 +146,7 @@ struct Control {
 	int n_dirty;                  // this pass: length of the dirty-row list
 	unsigned n_sel;               // this pass: targets the replacement visits
 	unsigned pad;
+	unsigned long long n_region;  // first pass: pixels of the noise-model sig_raw map (listed)
 	// Injected failures (0: none): the bound, in SM cycles, of one extra wait
 	// on a barrier that nothing completes, made by one warp of the first block
 	// of the bulk-staged prepare ([0]) and of the dense detection kernel ([1]).

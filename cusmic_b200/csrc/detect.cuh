@@ -520,7 +520,16 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
 	const bool err = has_error_map<PATH>(fd);
 	double v = INFINITY, nz = 0;
-	if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+	if (!LOW && !err && fresh && fd.sig_raw && x >= 2 && y >= 2 && x + 2 < w && y + 2 < h) {
+		// First pass, noise model: the window from the map region_sig_kernel
+		// wrote (every cell is within two of this HIGH pixel).
+		if (lane < 25) {
+			const long long i = (long long)(y + lane / 5 - 2) * w + x + lane % 5 - 2;
+			v = fd.sig_raw[i];
+			if (lane == 12)
+				nz = fd.noise[i];
+		}
+	} else if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
 		__syncwarp();
 		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
 		for (int k = lane; k < 81; k += 32)

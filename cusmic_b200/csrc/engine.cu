@@ -16,6 +16,7 @@
 #include "prepare_bulk.cuh"
 #include "incremental.cuh"
 #include "backward.cuh"
+#include "sigmap.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -420,6 +421,7 @@ struct Workspace {
 	DevBuf<unsigned> sel;   // targets the replacement after a pass visits
 	DevBuf<Seed> seeds;     // seed slots of the noise-model candidates
 	DevBuf<double> work;    // working pixels of the frames with a background
+	DevBuf<double> sigmap;  // first-pass sig_raw, then noise, of noise-model frames (2 x pixels)
 	DevBuf<uint2> cands;
 	DevBuf<int4> bulk;
 	DevBuf<int4> grow;
@@ -714,12 +716,17 @@ static void upload(Workspace &ws, Layout &L, cudaStream_t s, bool mapped = false
 		any_bg = any_bg || d.has_bg;
 	if (L.maxiter && any_bg)
 		ws.work.ensure(L.total_px);
+	if (L.maxiter && L.error_frames < (int)nf)
+		ws.sigmap.ensure(2 * L.total_px);
 	for (size_t f = 0; f < nf; ++f) {
 		L.frames[f].bits = L.maxiter ? ws.bits.p + L.bit_off[f] : nullptr;
 		L.frames[f].floors = L.maxiter ? ws.floors.p + L.thr_base[f] : nullptr;
 		L.frames[f].rowcand = L.maxiter ? ws.rowmarks.p + L.row_off[f] : nullptr;
 		L.frames[f].rowchg = L.maxiter ? ws.rowmarks.p + L.row_words + L.row_off[f] : nullptr;
 		L.frames[f].out = L.frames[f].clean;
+		const bool sm = L.maxiter && !L.frames[f].error;
+		L.frames[f].sig_raw = sm ? ws.sigmap.p + L.offsets[f] : nullptr;
+		L.frames[f].noise = sm ? ws.sigmap.p + L.total_px + L.offsets[f] : nullptr;
 		if (L.maxiter && L.frames[f].has_bg)
 			L.frames[f].clean = ws.work.p + L.offsets[f];
 	}
@@ -771,7 +778,7 @@ struct GraphLoop {
 
 // Kernel kinds reported by cusmic_plan_profile().
 enum KernelKind { K_INIT, K_PREPARE, K_FILL, K_SIGRAW, K_CAND, K_SEED, K_GROW, K_CONTROL,
-	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_CLASSIFY, K_FLOOR, K_RECLASS, K_DIRTY, K_KINDS };
+	K_REPLACE, K_RESTORE, K_COPY, K_LOW, K_CLASSIFY, K_FLOOR, K_RECLASS, K_DIRTY, K_SIGMAP, K_KINDS };
 
 // Optional CUDA-event timer: an event after every launch on the launching
 // stream, so each kernel's duration is the gap to the previous event.
@@ -842,6 +849,13 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 		classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
 			ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
 		mark(rec, K_CLASSIFY);
+		if (L.error_frames < nf) { // the noise-model candidates' sig_raw map
+			const int ng = (int)L.grow.size(), need = (ng + 7) / 8, gcap = di.sms * 8;
+			region_list_kernel<<<need < gcap ? need : gcap, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.grow.p,
+				ng, ws.ctl.p, ws.targets.p);
+			region_sig_kernel<<<di.sms * 8, 256, 0, s>>>(ws.frames.p, ws.targets.p, ws.ctl.p, L.prm);
+			mark(rec, K_SIGMAP);
+		}
 	}
 	// One launch per kind of frame in the batch: each variant compiles only
 	// its noise path (error map or noise model).  Error-map seeds are tested
@@ -1733,6 +1747,8 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 			L.frames[f].floors = p->L.frames[f].floors;
 			L.frames[f].rowcand = p->L.frames[f].rowcand;
 			L.frames[f].rowchg = p->L.frames[f].rowchg;
+			L.frames[f].sig_raw = p->L.frames[f].sig_raw;
+			L.frames[f].noise = p->L.frames[f].noise;
 			L.frames[f].out = L.frames[f].clean; // the new output buffer
 			if (p->L.frames[f].out != p->L.frames[f].clean) // working pixels in the workspace
 				L.frames[f].clean = p->L.frames[f].clean;
