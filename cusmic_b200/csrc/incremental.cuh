@@ -370,25 +370,44 @@ incremental_rows_kernel(const FrameDesc *__restrict__ frames, const int2 *__rest
 				if (MODEL) {
 					// Exact sig_raw of each pixel that passed, one at a time: its
 					// 5 x 5 window of clean one cell per lane, sorted across the
-					// warp (+inf padding), the median at rank 12.
-					for (int q = 0; q < todo; ++q) {
-						const int e = Q[q], kk = e >> 5, bit = e & 31;
-						const int px = 32 * (k0 + kk) + bit;
+					// warp (+inf padding), the median at rank 12.  The next
+					// pixel's window loads before this one's sort (one memory
+					// round trip per pixel hidden behind the previous sort), and
+					// an interior pixel's Laplacian comes from the window.
+					auto window_cell = [&](int q) {
 						double c = INFINITY;
-						if (lane < 25) {
+						if (q < todo && lane < 25) {
+							const int e = Q[q], px = 32 * (k0 + (e >> 5)) + (e & 31);
 							const int cx = px + lane % 5 - 2, cy = y + lane / 5 - 2;
 							c = cx >= 0 && cy >= 0 && cx < w && cy < fd.h
 								? fd.clean[(long long)cy * w + cx] : clean_at(fd, cx, cy, mode);
 						}
-						const double m = __shfl_sync(0xffffffffu, warp_sort32(c), 12);
+						return c;
+					};
+					double cur = window_cell(0);
+					for (int q = 0; q < todo; ++q) {
+						const double next = window_cell(q + 1);
+						const int e = Q[q], kk = e >> 5, bit = e & 31;
+						const int px = 32 * (k0 + kk) + bit;
+						const double ce = __shfl_sync(0xffffffffu, cur, 12);
+						const double up = __shfl_sync(0xffffffffu, cur, 7);
+						const double dn = __shfl_sync(0xffffffffu, cur, 17);
+						const double lf = __shfl_sync(0xffffffffu, cur, 11);
+						const double rt = __shfl_sync(0xffffffffu, cur, 13);
+						const double m = __shfl_sync(0xffffffffu, warp_sort32(cur), 12);
 						if (lane == 0) {
 							const long long i = (long long)y * w + px;
-							const double v = lap_at(fd, px, y, lm) / (2 * noise_from_median(fd, i, m));
+							// Interior: the four neighbours are in the frame, so
+							// the window holds the values lap_at reads.
+							const double lap = px >= 1 && y >= 1 && px + 1 < w && y + 1 < fd.h
+								? lap_formula(ce, up, dn, lf, rt) : lap_at(fd, px, y, lm);
+							const double v = lap / (2 * noise_from_median(fd, i, m));
 							if (v > prm.cr || v != v)
 								hmask[warp][kk] |= 1u << bit;
 							else if (v > prm.nb)
 								lmask[warp][kk] |= 1u << bit;
 						}
+						cur = next;
 					}
 				} else {
 					for (int q0 = 0; q0 < todo; q0 += 32) {
