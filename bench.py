@@ -62,6 +62,9 @@ SIG_BULK_DRAM_BYTES_PER_PX = 8.62
 # 565.2 MB read + 514.2 MB written over 67.1 Mpix (written pixels still in
 # L2 at the end of the launch are not counted).
 PREPARE_DRAM_BYTES_PER_PX = 16.08
+# ncu, prep_detect_kernel (prepare with the dense detection), one 16-frame
+# stack launch (this workload); None until captured.
+PREP_DETECT_DRAM_BYTES_PER_PX = None
 REF_GPU_SO = ROOT / "oracle" / "_ref" / "libcusmic_ref.so"
 
 
@@ -345,18 +348,23 @@ def main():
     # The dominant kernel: prepare (holes, exclusions, clean pixels and the
     # static bit planes, once per call), HBM-bound.  Per pixel it reads the
     # float64 input (8 B) and the mask byte (1 B), writes clean (8 B) and the
-    # HOLE, EXCL and DONOR bit words (3/8 B).  This batch's frames (widths a
-    # multiple of 16, aligned buffers, no background map) take the bulk-staged
-    # variant.
+    # HOLE, EXCL and DONOR bit words (3/8 B).  This batch's frames (error
+    # maps, widths a multiple of 16, aligned buffers, no background) take
+    # prep_detect_kernel, which also runs the first pass's dense detection on
+    # the input rows (no separate dense-detection launch, no re-read of the
+    # clean pixels; its pre-list writes, 16 B per listed pixel, about 1% of
+    # the pixels, are not counted); other batches the bulk-staged prepare.
+    fused = klaunch["sigraw"] == 0
     prep_px = nf * h * w * klaunch["prepare"]
     prep_bytes = prep_px * (8 + 1 + 8 + 3 / 8)
     prep_ms = kms["prepare"]
     prep_achieved = prep_bytes / (prep_ms / 1e3) / 1e9
     prep_launch_px = prep_px / max(1, klaunch["prepare"])
-    roofline = {"bound": "hbm", "kernel": "prepare_bulk_kernel",
+    dram_px = PREP_DETECT_DRAM_BYTES_PER_PX if fused else PREPARE_DRAM_BYTES_PER_PX
+    roofline = {"bound": "hbm", "kernel": "prep_detect_kernel" if fused else "prepare_bulk_kernel",
                 "achieved": round(prep_achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(prep_achieved / peak, 4),
-                "traffic": round(prep_launch_px * PREPARE_DRAM_BYTES_PER_PX),
+                "traffic": round(prep_launch_px * dram_px) if dram_px else None,
                 "peak_source": peak_source,
                 "algorithmic_bytes_per_launch": round(prep_bytes / max(1, klaunch["prepare"])),
                 "avg_launch_ms": round(prep_ms / max(1, klaunch["prepare"]), 4),
@@ -364,27 +372,32 @@ def main():
                 "kernel_share": {k: round(v / total_kernel_ms, 4) for k, v in kms.items() if v}}
 
     # Dense detection kernel (sig_bulk_kernel), run by the first (full) pass
-    # over every frame.  Per pixel it reads clean (8 B); its bit planes were
-    # zeroed by the call's prologue memset, and its writes (the sparse pre
-    # list) are a few MB.  The error map is not read there: its 32 x 32 block
-    # floors are computed once per call by floor_kernel.  Later passes are
-    # incremental and do not run it.
-    active_px = nf * h * w * klaunch["sigraw"]
-    detect_bytes = active_px * 8
-    detect_ms = kms["sigraw"]
-    achieved = detect_bytes / (detect_ms / 1e3) / 1e9
-    # DRAM bytes per active pixel of one launch from an ncu capture of the
-    # 4-frame stack, scaled to this launch's active pixels.
-    traffic = active_px * SIG_BULK_DRAM_BYTES_PER_PX / max(1, klaunch["sigraw"])
-    roofline_sig_bulk = {"bound": "hbm", "kernel": "sig_bulk_kernel", "achieved": round(achieved, 1),
-                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": round(traffic), "peak_source": peak_source,
-                         "algorithmic_bytes_per_launch": round(detect_bytes / max(1, klaunch["sigraw"])),
-                         "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4)}
+    # over every frame of batches that prep_detect_kernel does not serve (on
+    # this stack it is part of prepare; see roofline_sig_bulk_ragged).  Per
+    # pixel it reads clean (8 B); its bit planes were zeroed by the call's
+    # prologue memset, and its writes (the sparse pre list) are a few MB.  The
+    # error map is not read there: its 32 x 32 block floors are computed once
+    # per call by floor_kernel.  Later passes are incremental and do not run it.
+    roofline_sig_bulk = None
+    if not fused:
+        active_px = nf * h * w * klaunch["sigraw"]
+        detect_bytes = active_px * 8
+        detect_ms = kms["sigraw"]
+        achieved = detect_bytes / (detect_ms / 1e3) / 1e9
+        # DRAM bytes per active pixel of one launch from an ncu capture of the
+        # 4-frame stack, scaled to this launch's active pixels.
+        traffic = active_px * SIG_BULK_DRAM_BYTES_PER_PX / max(1, klaunch["sigraw"])
+        roofline_sig_bulk = {"bound": "hbm", "kernel": "sig_bulk_kernel",
+                             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "traffic": round(traffic),
+                             "peak_source": peak_source,
+                             "algorithmic_bytes_per_launch": round(
+                                 detect_bytes / max(1, klaunch["sigraw"])),
+                             "avg_launch_ms": round(detect_ms / max(1, klaunch["sigraw"]), 4)}
     # Kernels of one execution as the event profiler saw them, plus the one
     # that shares a mark with another kernel: the replacement's target
-    # selection (every pass).
-    launches_per_step = sum(klaunch.values()) + klaunch["sigraw"] + klaunch["dirty"]
+    # selection (every pass, as the loop control).
+    launches_per_step = sum(klaunch.values()) + klaunch["control"]
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -403,6 +416,16 @@ def main():
         out["plain"] = plain_vs_batched(plan, batch, stream, value / world, barrier)
         ragged, ragged_ctx = ragged_comparison(dev, stream, barrier)
         out["ragged"] = ragged
+        if out["roofline_sig_bulk"] is None and ragged["kernel_ms"].get("sigraw"):
+            # The dense kernel on the ragged batch (noise model): 8 B per pixel.
+            rb = ragged["pixels"] * 8
+            ach = rb / (ragged["kernel_ms"]["sigraw"] / 1e3) / 1e9
+            out["roofline_sig_bulk"] = {
+                "bound": "hbm", "kernel": "sig_bulk_kernel", "workload": "ragged_64",
+                "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": None, "peak_source": peak_source,
+                "algorithmic_bytes_per_launch": rb,
+                "avg_launch_ms": ragged["kernel_ms"]["sigraw"]}
         out["adjoint"], adjoint_ctx = adjoint_timing(dev, stream, barrier)
         out["reference_gpu"] = reference_gpu(plan, batch, ragged_ctx, adjoint_ctx, value,
                                              ragged["batched_mpix_s"], stream, dev)

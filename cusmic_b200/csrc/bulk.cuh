@@ -791,7 +791,8 @@ __device__ __forceinline__ void classify_flush(ClassifyStage &H, ClassifyStage &
 // with the error map or the exact noise model at the pixel: one warp per
 // consumer-warp region of an item, one lane per entry.  The high list grows
 // from the front of the candidate buffer, the low list from its back; a NaN
-// goes to the high list (the candidate kernel decides).
+// goes to the high list (the candidate kernel decides).  Error-map entries
+// listed with a bound of +inf get their exact Laplacian first.
 __global__ void __launch_bounds__(256, 4)
 classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const int4 *__restrict__ items, int nitems, const PreCand *__restrict__ pre,
@@ -826,7 +827,13 @@ classify_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restri
 					const PreCand pc = e[k0 + lane];
 					pix = pc.pixel;
 					if (fd.error) {
-						const double v = pc.lap / (2 * fd.error[pix]);
+						// A bound of +inf marks a pixel whose Laplacian reads a hole
+						// (prep_detect_kernel) or overflowed: the exact Laplacian of
+						// the filled working pixels.
+						const double lap = pc.lap != INFINITY ? pc.lap
+							: lap_at(fd, (int)(pix % (unsigned)fd.w), (int)(pix / (unsigned)fd.w),
+								lap_mode(prm.mode));
+						const double v = lap / (2 * fd.error[pix]);
 						cls = v > prm.cr || v != v ? 1 : v > prm.nb ? 2 : 0;
 					} else {
 						const int px = (int)(pix % (unsigned)fd.w), py = (int)(pix / (unsigned)fd.w);

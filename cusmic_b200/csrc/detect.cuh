@@ -114,6 +114,13 @@ __device__ __forceinline__ double clean_at(const FrameDesc &fd, int x, int y, in
 	return mx < 0 || my < 0 ? 0.0 : fd.clean[(long long)my * fd.w + mx];
 }
 
+// The Laplacian at an in-frame pixel (reference src/filters.cuh:98-104).
+__device__ __forceinline__ double lap_at(const FrameDesc &fd, int x, int y, int lm)
+{
+	return lap_formula(fd.clean[(long long)y * fd.w + x], clean_at(fd, x, y - 1, lm),
+		clean_at(fd, x, y + 1, lm), clean_at(fd, x - 1, y, lm), clean_at(fd, x + 1, y, lm));
+}
+
 // Noise model at an in-frame pixel from its 5 x 5 median of clean
 // (src/filters.cuh:107-123).
 __device__ __forceinline__ double noise_from_median(const FrameDesc &fd, long long i, double m)

@@ -14,6 +14,7 @@
 #include "bulk.cuh"
 #include "kernels.cuh"
 #include "prepare_bulk.cuh"
+#include "prep_detect.cuh"
 #include "incremental.cuh"
 #include "backward.cuh"
 #include "sigmap.cuh"
@@ -381,6 +382,10 @@ struct Layout {
 	DetectParams prm{};
 	int maxiter = 0;
 	int error_frames = 0; // frames with an error map (a rebound plan keeps which)
+	// Kernel choices that depend on the buffers' alignment (a rebound plan
+	// whose choices change is captured again): the bulk-staged prepare, and
+	// prepare with the dense detection in one kernel (prep_detect_kernel).
+	bool prep_bulk = false, fused = false;
 	cusmic_tuning tune{};
 	long long poison_wait[2] = {0, 0}; // injected failures in force when the batch was laid out
 };
@@ -569,6 +574,17 @@ static int item_rows(const cusmic_image *ims, size_t nf, int target_items)
 	return rows;
 }
 
+// The prepare kernels that suit every frame of a batch (see Layout).
+static void choose_kernels(Layout &L)
+{
+	L.prep_bulk = true;
+	L.fused = L.maxiter > 0;
+	for (const FrameDesc &fd : L.frames) {
+		L.prep_bulk = L.prep_bulk && prep_bulk_ok(fd);
+		L.fused = L.fused && prep_detect_ok(fd);
+	}
+}
+
 static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_options &o,
 	const cusmic_frame_scalars *sc, double *clean, uint8_t *mask, const DeviceInfo &di)
 {
@@ -653,6 +669,7 @@ static Layout make_layout(const cusmic_image *ims, size_t nf, const cusmic_optio
 				L.grow.push_back(make_int4((int)f, ty, k0, std::min(ty + GROW_ROWS, d.h)));
 	}
 	L.total_px = px;
+	choose_kernels(L);
 	L.row_words = (L.row_words + 3) & ~3ll;
 	// Planes padded to 4 words, so every plane starts on a 16-byte boundary.
 	L.plane_words = (words + 3) & ~3ll;
@@ -842,9 +859,12 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 				&ws.ctl.p->n_dirty, L.prm, ws.ctl.p, ws.cands.p);
 		mark(rec, K_RECLASS);
 	} else {
-		sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
-			ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
-		mark(rec, K_SIGRAW);
+		// (A fused batch's prologue listed the pixels already.)
+		if (!L.fused) {
+			sig_bulk_kernel<<<nbulk < cap ? nbulk : cap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
+				ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.pre.p, ws.pre_counts.p);
+			mark(rec, K_SIGRAW);
+		}
 		const int cgrid = (nbulk * BK_CWARPS + 7) / 8 < sparse ? (nbulk * BK_CWARPS + 7) / 8 : sparse;
 		classify_kernel<<<cgrid, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.bulk.p, nbulk, ws.pre.p,
 			ws.pre_counts.p, L.prm, ws.ctl.p, ws.cands.p);
@@ -903,11 +923,11 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 // (faster for error-map frames than any specialisation that was timed).
 static void launch_prepare(Workspace &ws, const Layout &L, const DeviceInfo &di, cudaStream_t s)
 {
-	bool model = true, bulk = true, rowmin = false, out = false;
+	bool model = true, rowmin = false, out = false;
+	const bool bulk = L.prep_bulk;
 	for (const FrameDesc &fd : L.frames) {
 		const int kind = prep_kind(fd);
 		model = model && kind == PREP_MODEL;
-		bulk = bulk && prep_bulk_ok(fd);
 		rowmin = rowmin || kind == PREP_MODEL || kind == PREP_MODEL_MAPS;
 		out = out || (fd.out && fd.out != fd.clean);
 	}
@@ -951,12 +971,29 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		P_ROWMIN == N_PLANES - 1, "plane order");
 	const long long z16 = (long long)(P_ROWMIN - P_CRMASK) * L.plane_words / 4;
 	const long long r16 = 2 * L.row_words / 4;
-	const long long zb = (z16 + 255) / 256, fb = (nf + 255) / 256, zcap = (long long)di.sms * 8;
+	const long long zb = (std::max(z16, r16) + 255) / 256, fb = (nf + 255) / 256,
+		zcap = (long long)di.sms * 8;
 	init_kernel<<<(int)std::max(fb, std::min(zb, zcap)), 256, 0, s>>>(ws.state.p, nf, ws.ctl.p,
 		L.maxiter, (unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1],
 		reinterpret_cast<uint4 *>(ws.bits.p + P_CRMASK * L.plane_words), z16,
 		reinterpret_cast<uint4 *>(ws.rowmarks.p), r16);
 	mark(rec, K_INIT); // the state and the zeroed planes
+	if (L.fused) {
+		// Error-map floors first (they read the maps only), then prepare with
+		// the first pass's dense detection in one kernel, then the hole fill.
+		const int nj = (int)L.jobs.size(), cap = di.sms * 8;
+		floor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p, ws.jobs.p,
+			nj, L.prm, ws.floors.p);
+		mark(rec, K_FLOOR);
+		const int nbulk = (int)L.bulk.size(), pcap = di.sms * PD_BLOCKS_PER_SM;
+		prep_detect_kernel<<<nbulk < pcap ? nbulk : pcap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.cands.p, ws.pre.p, ws.pre_counts.p);
+		mark(rec, K_PREPARE);
+		fill_list_kernel<<<di.sms * L.tune.sparse_blocks_per_sm, 256, 0, s>>>(ws.frames.p, ws.state.p,
+			ws.cands.p, &ws.ctl.p->n_holes);
+		mark(rec, K_FILL);
+		return;
+	}
 	launch_prepare(ws, L, di, s);
 	mark(rec, K_PREPARE);
 	// Block floors: error-map thresholds; noise-model keys from prepare's row
@@ -1755,11 +1792,23 @@ extern "C" int cusmic_plan_bind(cusmic_plan *p, const cusmic_image *ims, double 
 		}
 		p->ims.assign(ims, ims + nf);
 		p->L.frames = L.frames;
+		// New buffers can change which prepare kernels suit the batch: the
+		// graph is captured again with the new choice.
+		const bool recapture = L.prep_bulk != p->L.prep_bulk || L.fused != p->L.fused;
+		p->L.prep_bulk = L.prep_bulk;
+		p->L.fused = L.fused;
 		const size_t bytes = nf * sizeof(FrameDesc);
 		std::memcpy(p->ws.stage.p, p->L.frames.data(), bytes);
 		check(cudaMemcpyAsync(p->ws.frames.p, p->ws.stage.p, bytes, cudaMemcpyHostToDevice,
 			p->private_stream));
 		check(cudaStreamSynchronize(p->private_stream));
+		if (recapture && p->exec) {
+			cudaGraphExecDestroy(p->exec);
+			cudaGraphDestroy(p->graph);
+			p->exec = nullptr;
+			p->graph = nullptr;
+			capture_graph(*p);
+		}
 	}, msg, len);
 }
 

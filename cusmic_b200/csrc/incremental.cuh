@@ -81,13 +81,6 @@ __device__ __forceinline__ double block_threshold(const FrameDesc &fd, int bx, i
 	return tmin2 * (sqrt(rn * rn + g * m) / g);
 }
 
-// The Laplacian at an in-frame pixel (reference src/filters.cuh:98-104).
-__device__ __forceinline__ double lap_at(const FrameDesc &fd, int x, int y, int lm)
-{
-	return lap_formula(fd.clean[(long long)y * fd.w + x], clean_at(fd, x, y - 1, lm),
-		clean_at(fd, x, y + 1, lm), clean_at(fd, x - 1, y, lm), clean_at(fd, x + 1, y, lm));
-}
-
 __device__ __forceinline__ int wrap_index(int i, int n)
 {
 	i %= n;

@@ -107,7 +107,11 @@ cusmic_plan_passes(cusmic_plan *plan, int *passes);
  * grow/update, control, replace, restore, zero-iteration copy, low
  * candidates, classification of the dense pass's list, block floors, and of
  * the incremental passes the reclassification with work-list gather and the
- * dirty-row scan.  A timing aid; no counterpart in the reference. */
+ * dirty-row scan.  A batch whose frames all have an error map and no
+ * background, widths that are multiples of 16 and 16-byte aligned buffers
+ * runs prepare and the first pass's dense detection as one kernel, reported
+ * under prepare (no sig_raw launch).  A timing aid; no counterpart in the
+ * reference. */
 int
 cusmic_plan_profile(cusmic_plan *plan, void *stream, double *ms, int *launches, int kinds,
 	char *msg, size_t message_size);
