@@ -63,8 +63,9 @@ SIG_BULK_DRAM_BYTES_PER_PX = 8.62
 # L2 at the end of the launch are not counted).
 PREPARE_DRAM_BYTES_PER_PX = 16.08
 # ncu, prep_detect_kernel (prepare with the dense detection), one 16-frame
-# stack launch (this workload); None until captured.
-PREP_DETECT_DRAM_BYTES_PER_PX = None
+# stack launch (this workload): 601.2 MB read + 525.2 MB written over
+# 67.1 Mpix.
+PREP_DETECT_DRAM_BYTES_PER_PX = 16.79
 REF_GPU_SO = ROOT / "oracle" / "_ref" / "libcusmic_ref.so"
 
 
