@@ -9,7 +9,8 @@
   flags (``-std=c++14 --fmad=false``, Makefile:100-103).  Nothing is copied:
   nvcc reads the reference tree directly.  The .so is git-ignored but travels
   with the working tree to a GPU machine, where GPU tests use it as a second,
-  independent oracle.  Without the reference tree this step is skipped.
+  independent oracle.  The reference's ``src`` directory is given as an
+  argument or by ``CUSMIC_REFERENCE_SRC``; without it this step is skipped.
 
 Run ``python oracle/build.py`` or call the functions; both are idempotent.
 """
@@ -23,7 +24,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REFERENCE_SO = HERE / "_ref" / "libcusmic_ref.so"
-REFERENCE_SRC = Path(os.environ.get("CUSMIC_REFERENCE_SRC", "/root/reference/src"))
+REFERENCE_ENV = "CUSMIC_REFERENCE_SRC"  # the reference's src directory
 
 
 def _stale(target, sources):
@@ -44,24 +45,28 @@ def build_oracle(force=False):
     return ORACLE_SO
 
 
-def build_reference(force=False):
-    """Compile the reference CUDA library; returns its path or None."""
-    api = REFERENCE_SRC / "api.cu"
-    if not api.exists():
+def build_reference(src=None, force=False):
+    """Compile the reference CUDA library from the reference's ``src``
+    directory (argument, else $CUSMIC_REFERENCE_SRC); returns its path or None."""
+    src = src or os.environ.get(REFERENCE_ENV)
+    api = Path(src) / "api.cu" if src else None
+    if api is None or not api.exists():
         return REFERENCE_SO if REFERENCE_SO.exists() else None
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    sources = [api, *REFERENCE_SRC.glob("*.cuh"), *REFERENCE_SRC.glob("*.h")]
+    ref_src = api.parent
+    sources = [api, *ref_src.glob("*.cuh"), *ref_src.glob("*.h")]
     if force or _stale(REFERENCE_SO, sources):
         REFERENCE_SO.parent.mkdir(parents=True, exist_ok=True)
         cmd = [nvcc, "-std=c++14", "--fmad=false", "--cudart=static", "-O2",
                "-gencode", "arch=compute_100a,code=sm_100a",
                "-Xcompiler=-fPIC,-ffp-contract=off",
                '-DCUSMIC_VERSION="reference-oracle"',
-               f"-I{REFERENCE_SRC}", "--shared", str(api), "-o", str(REFERENCE_SO)]
+               f"-I{ref_src}", "--shared", str(api), "-o", str(REFERENCE_SO)]
         subprocess.run(cmd, check=True)
     return REFERENCE_SO
 
 
 if __name__ == "__main__":
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
     print(build_oracle(force="--force" in sys.argv))
-    print(build_reference(force="--force" in sys.argv))
+    print(build_reference(args[0] if args else None, force="--force" in sys.argv))

@@ -13,7 +13,8 @@ cannot travel with the tests, so this script stores what the tests need:
   that differ from the input, checked);
 * ``cleaned_sha256``: SHA-256 of the full cleaned float64 array.
 
-Usage: ``python tests/golden/make_golden.py [REFERENCE_TEST_DATA_DIR]``.
+Usage: ``python tests/golden/make_golden.py REFERENCE_TEST_DATA_DIR`` (the
+reference's ``test/data`` directory).
 """
 
 import gzip
@@ -86,4 +87,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/test/data")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference test/data directory>")
+    main(sys.argv[1])
