@@ -803,57 +803,173 @@ replace_select_kernel(const FrameDesc *__restrict__ frames, const FrameState *__
 	}
 }
 
-// Replacement after a pass, one warp per target: the targets listed in sel
-// (with radius: each replacement's window radius is kept), or with sel null
-// every target of the frames whose pass flagged new pixels.
-//
-// With fd.rowchg, a target whose value changed (bit for bit) gets its CHG
-// bit and its row mark: the next incremental pass starts from those pixels.
+// Bits of columns x - 2 .. x + 2 of row y of a bit plane (bit i: column
+// x - 2 + i; columns outside the frame read as zero: the words' padding bits
+// are zero, and words before the row's first or after its last read as zero).
+__device__ __forceinline__ uint32_t bits5(const uint32_t *plane, int words, int x, int y)
+{
+	const int a = x - 2, k = a >> 5; // k >= -1
+	const uint32_t *row = plane + (long long)y * words;
+	const uint32_t lo = k >= 0 ? row[k] : 0u, hi = k + 1 < words ? row[k + 1] : 0u;
+	return (uint32_t)((((unsigned long long)hi << 32) | lo) >> (a - 32 * k)) & 0x1fu;
+}
+
+// replace_one's first window (radius 2, clipped to the frame: at most 25
+// cells) evaluated by one thread: the donor bits of its five rows, the
+// donors' values, a sorting network over the 25 cells (non-donors as +inf)
+// and the same median (rank (nd - 1) / 2, or the midpoint of ranks
+// (nd - 1) / 2 and nd / 2).  Equal nonzero donors are the same bits, and an
+// odd count's 0.0 + lo drops a zero's sign, so any sort gives the bits of
+// replace_one's exchange network except when an even count's two middle
+// values are zeros and the window holds zeros of both signs.  Returns false
+// for that window and for one without a donor: the caller's warp then runs
+// replace_one (the exchange network, expanding windows).
+__device__ __forceinline__ bool first_window_value(const FrameDesc &fd, int x, int y, double &out)
+{
+	const int w = fd.w, h = fd.h, words = fd.words;
+	const uint32_t *don = plane_ptr(fd, P_DONOR), *crm = plane_ptr(fd, P_CRMASK);
+	uint32_t rb[5];
+	int nd = 0;
+#pragma unroll
+	for (int dy = 0; dy < 5; ++dy) {
+		const int yy = y - 2 + dy;
+		rb[dy] = yy >= 0 && yy < h ? bits5(don, words, x, yy) & ~bits5(crm, words, x, yy) : 0u;
+		nd += __popc(rb[dy]);
+	}
+	if (nd == 0)
+		return false;
+	double v[25];
+	bool pz = false, nz = false; // donors of +0 and of -0
+#pragma unroll
+	for (int c = 0; c < 25; ++c) {
+		const int dy = c / 5, dx = c % 5;
+		v[c] = INFINITY;
+		if ((rb[dy] >> dx) & 1u) {
+			v[c] = fd.clean[(long long)(y - 2 + dy) * w + (x - 2 + dx)];
+			pz |= v[c] == 0 && !signbit(v[c]);
+			nz |= v[c] == 0 && signbit(v[c]);
+		}
+	}
+	sort_network(v);
+	const int k1 = (nd - 1) / 2, k2 = nd / 2;
+	double lo = 0, hi = 0;
+#pragma unroll
+	for (int c = 0; c < 25; ++c) {
+		lo = c == k1 ? v[c] : lo;
+		hi = c == k2 ? v[c] : hi;
+	}
+	if (!(nd % 2) && lo == 0 && hi == 0 && pz && nz)
+		return false;
+	out = nd % 2 ? 0.0 + lo : midpoint(lo, hi);
+	return true;
+}
+
+// The bookkeeping of a target's replacement: its window radius, and with
+// fd.rowchg, when its value changed (bit for bit), its CHG bit and its row
+// mark (the next incremental pass starts from those pixels).
+__device__ __forceinline__ void replaced(const FrameDesc &fd, int x, int y, long long e, int r, bool changed,
+	uint8_t *radius)
+{
+	if (radius)
+		radius[e] = (uint8_t)(r < 255 ? r : 255);
+	if (changed && fd.rowchg) {
+		atomicOr(plane_ptr(fd, P_CHG) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
+		fd.rowchg[y] = 1u;
+	}
+}
+
+// Replacement after a pass (src/replace.cuh:111-153): the targets listed in
+// sel (with radius: each replacement's window radius is kept), or with sel
+// null every target of the frames whose pass flagged new pixels.  A thread
+// per target evaluates its first window (first_window_value); the warp
+// replaces the targets it leaves, one after another, with replace_one.
+// Targets are in the mask, so never donors: no target reads another's value.
 __global__ void __launch_bounds__(256)
 replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const uint2 *__restrict__ list, const unsigned long long *count, const unsigned *sel,
 	const unsigned *nsel, uint8_t *radius)
 {
 	const int lane = threadIdx.x & 31;
-	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
 	const long long n = sel ? (long long)*nsel : (long long)*count;
-	for (long long s = gw; s < n; s += nw) {
-		const long long e = sel ? (long long)sel[s] : s;
-		const uint2 t = list[e];
-		if (!sel && !state[t.x].replace)
-			continue; // warp-uniform
-		const FrameDesc &fd = frames[t.x];
-		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
-		bool ch = false;
-		const int r = replace_one(fd, x, y, &ch);
-		if (lane == 0) {
-			if (radius)
-				radius[e] = (uint8_t)(r < 255 ? r : 255);
-			if (ch && fd.rowchg) {
-				atomicOr(plane_ptr(fd, P_CHG) + (long long)y * fd.words + (x >> 5), 1u << (x & 31));
-				fd.rowchg[y] = 1u;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+	     base += stride) { // warp-uniform
+		const long long s = base + lane;
+		long long e = 0;
+		uint2 t = make_uint2(0u, 0u);
+		bool defer = false;
+		if (s < n) {
+			e = sel ? (long long)sel[s] : s;
+			t = list[e];
+			if (sel || state[t.x].replace) {
+				const FrameDesc &fd = frames[t.x];
+				const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+				double v;
+				if (first_window_value(fd, x, y, v)) {
+					double &dst = fd.clean[(long long)y * fd.w + x];
+					const bool ch = __double_as_longlong(dst) != __double_as_longlong(v);
+					dst = v;
+					// Keep the block's floor a lower bound of its clean values.
+					if (fd.floors && !fd.error)
+						atomicMin(&fd.floors[(y >> 5) * ((fd.w + 31) >> 5) + (x >> 5)].key, order_key(v));
+					replaced(fd, x, y, e, 2, ch, radius);
+				} else {
+					defer = true;
+				}
 			}
+		}
+		for (unsigned m = __ballot_sync(0xffffffffu, defer); m; m &= m - 1) {
+			const int j = __ffs(m) - 1;
+			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
+			const long long ej = __shfl_sync(0xffffffffu, e, j);
+			const FrameDesc &fd = frames[tj.x];
+			const int x = (int)(tj.y % (unsigned)fd.w), y = (int)(tj.y / (unsigned)fd.w);
+			bool ch = false;
+			const int r = replace_one(fd, x, y, &ch);
+			if (lane == 0)
+				replaced(fd, x, y, ej, r, ch, radius);
 		}
 	}
 }
 
 // Initial fill of non-finite pixels (src/cleaner.cuh:78-100) for frames with
-// a finite donor, from the hole list prepare_kernel wrote: one warp per hole
-// (holes are never donors, so the order does not matter).
+// a finite donor, from the hole list prepare wrote (holes are never donors, so
+// the order does not matter): a thread per hole (first_window_value), the
+// warp for the holes it leaves.
 __global__ void __launch_bounds__(256)
 fill_list_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const uint2 *__restrict__ holes, const unsigned long long *count)
 {
-	const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	const int lane = threadIdx.x & 31;
 	const long long n = (long long)*count;
-	for (long long e = gw; e < n; e += nw) {
-		const uint2 t = holes[e];
-		if (!state[t.x].finite)
-			continue; // warp-uniform
-		const FrameDesc &fd = frames[t.x];
-		replace_one(fd, (int)(t.y % (unsigned)fd.w), (int)(t.y / (unsigned)fd.w));
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+	     base += stride) { // warp-uniform
+		const long long e = base + lane;
+		uint2 t = make_uint2(0u, 0u);
+		bool defer = false;
+		if (e < n) {
+			t = holes[e];
+			if (state[t.x].finite) {
+				const FrameDesc &fd = frames[t.x];
+				const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+				double r;
+				if (first_window_value(fd, x, y, r)) {
+					fd.clean[(long long)y * fd.w + x] = r;
+					// Keep the block's floor a lower bound of its clean values.
+					if (fd.floors && !fd.error)
+						atomicMin(&fd.floors[(y >> 5) * ((fd.w + 31) >> 5) + (x >> 5)].key, order_key(r));
+				} else {
+					defer = true;
+				}
+			}
+		}
+		for (unsigned m = __ballot_sync(0xffffffffu, defer); m; m &= m - 1) {
+			const int j = __ffs(m) - 1;
+			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
+			const FrameDesc &fd = frames[tj.x];
+			replace_one(fd, (int)(tj.y % (unsigned)fd.w), (int)(tj.y / (unsigned)fd.w));
+		}
 	}
 }
 

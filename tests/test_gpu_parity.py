@@ -682,3 +682,22 @@ def test_large_replacement_windows(cuda, oracle, seed):
     if "gain" in frame:
         opts.update(gain=1.5, readnoise=0.5)
     check_against_oracle(oracle, [frame], opts)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("w", (64, 61))
+def test_hole_fill_signed_zero_donors(cuda, oracle, mode, w):
+    """Isolated holes (2% NaN, some on edges and corners) on a field of +0, -0
+    and 1.0 with masked pixels, so first fill windows hold even and odd donor
+    counts whose middle values are zeros of either sign: the per-hole fill
+    must give the reference's bits (the exchange network decides which zero a
+    tie yields; windows with both signs are left to it), with width 64 for the
+    fused prepare and 61 for the two-kernel path."""
+    rng = np.random.default_rng(9100 + w + MODES.index(mode))
+    h = 40
+    data = rng.choice(np.array([0.0, -0.0, 1.0]), size=(h, w), p=[0.4, 0.4, 0.2])
+    data[rng.random((h, w)) < 0.02] = np.nan
+    data[0, 0] = data[h - 1, w - 1] = data[0, w - 1] = np.nan
+    mask = rng.random((h, w)) < 0.15
+    frame = dict(data=data, mask=mask, error=np.full((h, w), 0.4))
+    check_against_oracle(oracle, [frame], dict(SETTINGS, maxiter=2, border=mode))
