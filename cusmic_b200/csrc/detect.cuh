@@ -527,16 +527,7 @@ __device__ __forceinline__ double candidate_sig(const FrameDesc &fd, int x, int 
 	const int w = fd.w, h = fd.h, mode = prm.mode, lm = lap_mode(mode);
 	const bool err = has_error_map<PATH>(fd);
 	double v = INFINITY, nz = 0;
-	if (!LOW && !err && fresh && fd.sig_raw && x >= 2 && y >= 2 && x + 2 < w && y + 2 < h) {
-		// First pass, noise model: the window from the map region_sig_kernel
-		// wrote (every cell is within two of this HIGH pixel).
-		if (lane < 25) {
-			const long long i = (long long)(y + lane / 5 - 2) * w + x + lane % 5 - 2;
-			v = fd.sig_raw[i];
-			if (lane == 12)
-				nz = fd.noise[i];
-		}
-	} else if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
+	if (x >= 4 && y >= 4 && x + 4 < w && y + 4 < h) { // warp-uniform
 		__syncwarp();
 		const double *src = fd.clean + (long long)(y - 4) * w + (x - 4);
 		for (int k = lane; k < 81; k += 32)
@@ -617,6 +608,41 @@ __device__ __forceinline__ void candidate_eval(const FrameDesc &fd, uint2 t, lon
 	}
 }
 
+// The first pass's evaluation of a noise-model candidate at least two pixels
+// from every edge by one thread: its 25 window values from the sig_raw map
+// (region_sig_kernel), their median by a sorting network (NaN-free windows:
+// any network gives the median's value, a zero's sign aside, which no
+// threshold sees), the S1 / S2 bits and the seed slot, as candidate_eval.
+// Returns false for a window holding a NaN (the warp's NaN rule decides it).
+__device__ __forceinline__ bool map_candidate(const FrameDesc &fd, uint2 t, long long e, int x, int y,
+	const DetectParams &prm, Seed *seeds)
+{
+	const int w = fd.w;
+	double v[25];
+	bool nan = false;
+#pragma unroll
+	for (int c = 0; c < 25; ++c) {
+		v[c] = fd.sig_raw[(long long)(y + c / 5 - 2) * w + x + c % 5 - 2];
+		nan |= isnan(v[c]);
+	}
+	if (nan)
+		return false;
+	const long long word = (long long)y * fd.words + (x >> 5);
+	const uint32_t bit = 1u << (x & 31);
+	const bool hole = (plane_ptr(fd, P_HOLE)[word] & bit) != 0;
+	const uint32_t excl = plane_ptr(fd, P_EXCL)[word];
+	const double nz = fd.noise[(long long)y * w + x];
+	const double center = v[12];
+	const double sig = center - median_network(v);
+	if (!hole) { // a hole's significance is zero: no bit (the planes start zeroed)
+		write_bit(plane_ptr(fd, P_S2) + word, bit, sig > prm.nb, true);
+		write_bit(plane_ptr(fd, P_S1) + word, bit, sig > prm.cr, true);
+	}
+	const bool seed = !hole && sig > prm.cr && !(excl & bit);
+	seeds[e] = seed ? Seed{t.x, t.y, sig, nz} : Seed{NO_SEED, 0, 0.0, 0.0};
+	return true;
+}
+
 // B, high list: one warp per candidate.  Holes have sig = 0
 // (src/filters.cuh:137-146): no bit, no seed; the dense kernel does not test
 // the hole plane itself.
@@ -644,6 +670,48 @@ candidate_high_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restr
 		const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
 		const bool hole = test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
 		candidate_eval<false, PATH>(fd, t, e, x, y, P, S, prm, seeds, fresh != 0, hole);
+	}
+}
+
+// B, high list, first pass on noise-model frames: a thread per candidate
+// whose window the sig_raw map holds (map_candidate); the warp evaluates the
+// others (frame edges, windows with a NaN) one after another with
+// candidate_eval.  Its own launch bounds: the thread path holds 25 window
+// values, the warp path (candidate_high_kernel) runs at four blocks per SM.
+__global__ void __launch_bounds__(256, 2)
+candidate_map_kernel(const FrameDesc *__restrict__ frames, const uint2 *__restrict__ cands,
+	DetectParams prm, Control *ctl, Seed *seeds)
+{
+	constexpr int PATH = PATH_MODEL;
+	__shared__ double patches[8][81];
+	__shared__ double scratch[8][CS_RUNS];
+	double *P = patches[threadIdx.x >> 5], *S = scratch[threadIdx.x >> 5];
+	const long long n = (long long)ctl->n_cand;
+	const int lane = threadIdx.x & 31;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+	     base += stride) { // warp-uniform
+		const long long e = base + lane;
+		uint2 t = make_uint2(0u, 0u);
+		bool defer = false;
+		if (e < n) {
+			t = cands[e];
+			const FrameDesc &fd = frames[t.x];
+			if (serves<PATH>(fd)) {
+				const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
+				defer = !(fd.sig_raw && x >= 2 && y >= 2 && x + 2 < fd.w && y + 2 < fd.h &&
+					map_candidate(fd, t, e, x, y, prm, seeds));
+			}
+		}
+		for (unsigned m = __ballot_sync(0xffffffffu, defer); m; m &= m - 1) {
+			const int j = __ffs(m) - 1;
+			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j),
+				__shfl_sync(0xffffffffu, t.y, j));
+			const FrameDesc &fd = frames[tj.x];
+			const int x = (int)(tj.y % (unsigned)fd.w), y = (int)(tj.y / (unsigned)fd.w);
+			const bool hole = test_bit(plane_ptr(fd, P_HOLE), fd.words, x, y);
+			candidate_eval<false, PATH>(fd, tj, base + j, x, y, P, S, prm, seeds, true, hole);
+		}
 	}
 }
 

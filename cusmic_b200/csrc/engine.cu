@@ -884,9 +884,11 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	if (L.error_frames)
 		candidate_seed_kernel<PATH_ERROR><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
 			ws.ctl.p, model ? ws.seeds.p : nullptr, !incremental);
-	if (model)
+	if (model && incremental)
 		candidate_high_kernel<PATH_MODEL><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
-			ws.ctl.p, ws.seeds.p, !incremental);
+			ws.ctl.p, ws.seeds.p, 0);
+	else if (model) // the first pass: windows from the sig_raw map, a thread per candidate
+		candidate_map_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p, ws.seeds.p);
 	mark(rec, K_CAND);
 	if (model) {
 		seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p, !incremental);
