@@ -274,9 +274,8 @@ __device__ __forceinline__ bool thread_floor_job(const FloorJob &jb, const Frame
 	return jb.kind && !fd.gain_map && !fd.rn_map;
 }
 
-__global__ void __launch_bounds__(256)
-floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
-	DetectParams prm, BlockFloor *floors)
+__device__ __forceinline__ void floor_jobs(const FrameDesc *__restrict__ frames,
+	const FloorJob *__restrict__ jobs, int njobs, const DetectParams &prm, BlockFloor *floors)
 {
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -334,6 +333,13 @@ floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ 
 		if (lane == 0)
 			floors[jb.out].thr = T >= 0 ? T : 0.0; // NaN lists everything
 	}
+}
+
+__global__ void __launch_bounds__(256)
+floor_kernel(const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
+	DetectParams prm, BlockFloor *floors)
+{
+	floor_jobs(frames, jobs, njobs, prm, floors);
 }
 
 // Floors of the noise-model blocks of frames without gain or read-noise maps,

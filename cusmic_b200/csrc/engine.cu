@@ -829,6 +829,12 @@ static inline void mark(Recorder *r, int kind)
 		r->mark(kind);
 }
 
+// Grids of the kernels with a thread per work item (grid-stride loops): the
+// blocks that fit an SM at their register use (80 per thread for the
+// first-window kernels, 120 for candidate_map_kernel), so a short list costs
+// no waves of idle blocks.
+constexpr int WINDOW_BLOCKS_PER_SM = 3, MAP_BLOCKS_PER_SM = 2;
+
 // One detection pass.  The first pass of a call is full: the dense kernel
 // lists every candidate and the classification fills the HIGH / LOW planes.
 // Later passes are incremental (incremental.cuh): they start from the pixels
@@ -888,7 +894,8 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 		candidate_high_kernel<PATH_MODEL><<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
 			ws.ctl.p, ws.seeds.p, 0);
 	else if (model) // the first pass: windows from the sig_raw map, a thread per candidate
-		candidate_map_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm, ws.ctl.p, ws.seeds.p);
+		candidate_map_kernel<<<di.sms * MAP_BLOCKS_PER_SM, 256, 0, s>>>(ws.frames.p, ws.cands.p, L.prm,
+			ws.ctl.p, ws.seeds.p);
 	mark(rec, K_CAND);
 	if (model) {
 		seed_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.seeds.p, L.prm, ws.ctl.p, !incremental);
@@ -914,7 +921,7 @@ static void launch_pass(Workspace &ws, const Layout &L, const DeviceInfo &di, cu
 	replace_select_kernel<<<tb, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
 		&ws.ctl.p->n_targets, ws.radius.p, ws.ctl.p, ws.sel.p,
 		reinterpret_cast<uint4 *>(ws.rowmarks.p + L.row_words), L.row_words / 4);
-	replace_kernel<<<sparse, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
+	replace_kernel<<<di.sms * WINDOW_BLOCKS_PER_SM, 256, 0, s>>>(ws.frames.p, ws.state.p, ws.targets.p,
 		&ws.ctl.p->n_targets, ws.sel.p, &ws.ctl.p->n_sel, ws.radius.p);
 	mark(rec, K_REPLACE);
 }
@@ -975,27 +982,31 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 	const long long r16 = 2 * L.row_words / 4;
 	const long long zb = (std::max(z16, r16) + 255) / 256, fb = (nf + 255) / 256,
 		zcap = (long long)di.sms * 8;
-	init_kernel<<<(int)std::max(fb, std::min(zb, zcap)), 256, 0, s>>>(ws.state.p, nf, ws.ctl.p,
-		L.maxiter, (unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1],
-		reinterpret_cast<uint4 *>(ws.bits.p + P_CRMASK * L.plane_words), z16,
-		reinterpret_cast<uint4 *>(ws.rowmarks.p), r16);
-	mark(rec, K_INIT); // the state and the zeroed planes
+	uint4 *const zero = reinterpret_cast<uint4 *>(ws.bits.p + P_CRMASK * L.plane_words);
+	uint4 *const zero2 = reinterpret_cast<uint4 *>(ws.rowmarks.p);
 	if (L.fused) {
-		// Error-map floors first (they read the maps only), then prepare with
-		// the first pass's dense detection in one kernel, then the hole fill.
-		const int nj = (int)L.jobs.size(), cap = di.sms * 8;
-		floor_kernel<<<(nj + 7) / 8 < cap ? (nj + 7) / 8 : cap, 256, 0, s>>>(ws.frames.p, ws.jobs.p,
-			nj, L.prm, ws.floors.p);
-		mark(rec, K_FLOOR);
+		// The error-map floors (they read the maps only) in the same launch
+		// as the state and the zeroing, then prepare with the first pass's
+		// dense detection in one kernel, then the hole fill.
+		const long long jb = ((long long)L.jobs.size() + 7) / 8;
+		prep_init_kernel<<<(int)std::max({fb, std::min(zb, zcap), std::min(jb, zcap)}), 256, 0, s>>>(
+			ws.state.p, nf, ws.ctl.p, L.maxiter, (unsigned long long)L.total_px, L.poison_wait[0],
+			L.poison_wait[1], zero, z16, zero2, r16, ws.frames.p, ws.jobs.p, (int)L.jobs.size(), L.prm,
+			ws.floors.p);
+		mark(rec, K_INIT); // the state, the zeroed planes and the floors
 		const int nbulk = (int)L.bulk.size(), pcap = di.sms * PD_BLOCKS_PER_SM;
 		prep_detect_kernel<<<nbulk < pcap ? nbulk : pcap, BK_THREADS, 0, s>>>(ws.frames.p, ws.state.p,
 			ws.bulk.p, nbulk, L.prm, ws.ctl.p, ws.cands.p, ws.pre.p, ws.pre_counts.p);
 		mark(rec, K_PREPARE);
-		fill_list_kernel<<<di.sms * L.tune.sparse_blocks_per_sm, 256, 0, s>>>(ws.frames.p, ws.state.p,
+		fill_list_kernel<<<di.sms * WINDOW_BLOCKS_PER_SM, 256, 0, s>>>(ws.frames.p, ws.state.p,
 			ws.cands.p, &ws.ctl.p->n_holes);
 		mark(rec, K_FILL);
 		return;
 	}
+	init_kernel<<<(int)std::max(fb, std::min(zb, zcap)), 256, 0, s>>>(ws.state.p, nf, ws.ctl.p,
+		L.maxiter, (unsigned long long)L.total_px, L.poison_wait[0], L.poison_wait[1], zero, z16, zero2,
+		r16);
+	mark(rec, K_INIT); // the state and the zeroed planes
 	launch_prepare(ws, L, di, s);
 	mark(rec, K_PREPARE);
 	// Block floors: error-map thresholds; noise-model keys from prepare's row
@@ -1011,7 +1022,7 @@ static void launch_prologue(Workspace &ws, const Layout &L, const DeviceInfo &di
 		mark(rec, K_FLOOR);
 	}
 	// The hole list lives in the candidate buffer until the first pass.
-	fill_list_kernel<<<di.sms * L.tune.sparse_blocks_per_sm, 256, 0, s>>>(ws.frames.p, ws.state.p,
+	fill_list_kernel<<<di.sms * WINDOW_BLOCKS_PER_SM, 256, 0, s>>>(ws.frames.p, ws.state.p,
 		ws.cands.p, &ws.ctl.p->n_holes);
 	mark(rec, K_FILL);
 }

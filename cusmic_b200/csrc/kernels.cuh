@@ -91,9 +91,9 @@ validate_kernel(const double *__restrict__ v, long long n, int minimum, unsigned
 // Per-frame state and loop control of a call; with `zero`, also zeroes the n16
 // 16-byte words at zero (the bit planes that nothing writes before the first
 // pass, and the row marks) with a grid-stride loop of 16-byte stores.
-__global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
-	unsigned long long cand_cap, long long poison_prepare = 0, long long poison_detect = 0,
-	uint4 *zero = nullptr, long long n16 = 0, uint4 *zero2 = nullptr, long long n16b = 0)
+__device__ __forceinline__ void init_state(FrameState *state, int nf, Control *ctl, int maxiter,
+	unsigned long long cand_cap, long long poison_prepare, long long poison_detect, uint4 *zero,
+	long long n16, uint4 *zero2, long long n16b)
 {
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n16; j += stride)
@@ -115,6 +115,13 @@ __global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter
 		c.poison_wait[1] = poison_detect;
 		*ctl = c;
 	}
+}
+
+__global__ void init_kernel(FrameState *state, int nf, Control *ctl, int maxiter,
+	unsigned long long cand_cap, long long poison_prepare = 0, long long poison_detect = 0,
+	uint4 *zero = nullptr, long long n16 = 0, uint4 *zero2 = nullptr, long long n16b = 0)
+{
+	init_state(state, nf, ctl, maxiter, cand_cap, poison_prepare, poison_detect, zero, n16, zero2, n16b);
 }
 
 // IEEE bits mapped to an unsigned total order (reference src/replace.cuh:37-48).

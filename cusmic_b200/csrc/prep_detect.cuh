@@ -403,6 +403,20 @@ __device__ __forceinline__ bool pd_consumer(BulkRing &R, const uint8_t (*M)[BK_C
 	return ok;
 }
 
+// The call's first launch on a batch prep_detect_kernel serves: init_kernel's
+// state, control and plane zeroing, and in the same grid the error maps'
+// block floors (floor_kernel's jobs, which read the maps only), so the floors
+// need no launch of their own and overlap the zeroing.
+__global__ void __launch_bounds__(256)
+prep_init_kernel(FrameState *state, int nf, Control *ctl, int maxiter, unsigned long long cand_cap,
+	long long poison_prepare, long long poison_detect, uint4 *zero, long long n16, uint4 *zero2,
+	long long n16b, const FrameDesc *__restrict__ frames, const FloorJob *__restrict__ jobs, int njobs,
+	DetectParams prm, BlockFloor *floors)
+{
+	init_state(state, nf, ctl, maxiter, cand_cap, poison_prepare, poison_detect, zero, n16, zero2, n16b);
+	floor_jobs(frames, jobs, njobs, prm, floors);
+}
+
 __global__ void __launch_bounds__(BK_THREADS, PD_BLOCKS_PER_SM)
 prep_detect_kernel(const FrameDesc *__restrict__ frames, FrameState *state, const int4 *__restrict__ items,
 	int nitems, DetectParams prm, Control *ctl, uint2 *holes, PreCand *pre, int *pre_counts)
