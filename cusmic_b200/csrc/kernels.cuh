@@ -885,29 +885,37 @@ __device__ __forceinline__ void replaced(const FrameDesc &fd, int x, int y, long
 	}
 }
 
+// Items the thread path of a block leaves, replaced by all of its warps.
+struct WindowQueue {
+	long long e[256];
+	int n;
+};
+
 // Replacement after a pass (src/replace.cuh:111-153): the targets listed in
 // sel (with radius: each replacement's window radius is kept), or with sel
 // null every target of the frames whose pass flagged new pixels.  A thread
-// per target evaluates its first window (first_window_value); the warp
-// replaces the targets it leaves, one after another, with replace_one.
+// per target evaluates its first window (first_window_value); the targets it
+// leaves (windows inside a cluster of flagged pixels) are queued in shared
+// memory and the block's warps replace them with replace_one, spread over all
+// eight warps so that a cluster does not hold one warp for many targets.
 // Targets are in the mask, so never donors: no target reads another's value.
 __global__ void __launch_bounds__(256)
 replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const uint2 *__restrict__ list, const unsigned long long *count, const unsigned *sel,
 	const unsigned *nsel, uint8_t *radius)
 {
-	const int lane = threadIdx.x & 31;
+	__shared__ WindowQueue Q;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	const long long n = sel ? (long long)*nsel : (long long)*count;
 	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
-	     base += stride) { // warp-uniform
-		const long long s = base + lane;
-		long long e = 0;
-		uint2 t = make_uint2(0u, 0u);
-		bool defer = false;
+	if (threadIdx.x == 0)
+		Q.n = 0;
+	__syncthreads();
+	for (long long base = blockIdx.x * (long long)blockDim.x; base < n; base += stride) { // block-uniform
+		const long long s = base + threadIdx.x;
 		if (s < n) {
-			e = sel ? (long long)sel[s] : s;
-			t = list[e];
+			const long long e = sel ? (long long)sel[s] : s;
+			const uint2 t = list[e];
 			if (sel || state[t.x].replace) {
 				const FrameDesc &fd = frames[t.x];
 				const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
@@ -921,42 +929,48 @@ replace_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restric
 						atomicMin(&fd.floors[(y >> 5) * ((fd.w + 31) >> 5) + (x >> 5)].key, order_key(v));
 					replaced(fd, x, y, e, 2, ch, radius);
 				} else {
-					defer = true;
+					Q.e[atomicAdd(&Q.n, 1)] = e;
 				}
 			}
 		}
-		for (unsigned m = __ballot_sync(0xffffffffu, defer); m; m &= m - 1) {
-			const int j = __ffs(m) - 1;
-			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
-			const long long ej = __shfl_sync(0xffffffffu, e, j);
-			const FrameDesc &fd = frames[tj.x];
-			const int x = (int)(tj.y % (unsigned)fd.w), y = (int)(tj.y / (unsigned)fd.w);
+		__syncthreads();
+		const int nq = Q.n;
+		for (int q = warp; q < nq; q += nwarps) {
+			const long long e = Q.e[q];
+			const uint2 t = list[e];
+			const FrameDesc &fd = frames[t.x];
+			const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
 			bool ch = false;
 			const int r = replace_one(fd, x, y, &ch);
 			if (lane == 0)
-				replaced(fd, x, y, ej, r, ch, radius);
+				replaced(fd, x, y, e, r, ch, radius);
 		}
+		__syncthreads();
+		if (threadIdx.x == 0)
+			Q.n = 0;
+		__syncthreads();
 	}
 }
 
 // Initial fill of non-finite pixels (src/cleaner.cuh:78-100) for frames with
 // a finite donor, from the hole list prepare wrote (holes are never donors, so
 // the order does not matter): a thread per hole (first_window_value), the
-// warp for the holes it leaves.
+// block's warps for the holes it leaves (replace_kernel's queue).
 __global__ void __launch_bounds__(256)
 fill_list_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restrict__ state,
 	const uint2 *__restrict__ holes, const unsigned long long *count)
 {
-	const int lane = threadIdx.x & 31;
+	__shared__ WindowQueue Q;
+	const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	const long long n = (long long)*count;
 	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
-	     base += stride) { // warp-uniform
-		const long long e = base + lane;
-		uint2 t = make_uint2(0u, 0u);
-		bool defer = false;
+	if (threadIdx.x == 0)
+		Q.n = 0;
+	__syncthreads();
+	for (long long base = blockIdx.x * (long long)blockDim.x; base < n; base += stride) { // block-uniform
+		const long long e = base + threadIdx.x;
 		if (e < n) {
-			t = holes[e];
+			const uint2 t = holes[e];
 			if (state[t.x].finite) {
 				const FrameDesc &fd = frames[t.x];
 				const int x = (int)(t.y % (unsigned)fd.w), y = (int)(t.y / (unsigned)fd.w);
@@ -967,16 +981,21 @@ fill_list_kernel(const FrameDesc *__restrict__ frames, const FrameState *__restr
 					if (fd.floors && !fd.error)
 						atomicMin(&fd.floors[(y >> 5) * ((fd.w + 31) >> 5) + (x >> 5)].key, order_key(r));
 				} else {
-					defer = true;
+					Q.e[atomicAdd(&Q.n, 1)] = e;
 				}
 			}
 		}
-		for (unsigned m = __ballot_sync(0xffffffffu, defer); m; m &= m - 1) {
-			const int j = __ffs(m) - 1;
-			const uint2 tj = make_uint2(__shfl_sync(0xffffffffu, t.x, j), __shfl_sync(0xffffffffu, t.y, j));
-			const FrameDesc &fd = frames[tj.x];
-			replace_one(fd, (int)(tj.y % (unsigned)fd.w), (int)(tj.y / (unsigned)fd.w));
+		__syncthreads();
+		const int nq = Q.n;
+		for (int q = warp; q < nq; q += nwarps) {
+			const uint2 t = holes[Q.e[q]];
+			const FrameDesc &fd = frames[t.x];
+			replace_one(fd, (int)(t.y % (unsigned)fd.w), (int)(t.y / (unsigned)fd.w));
 		}
+		__syncthreads();
+		if (threadIdx.x == 0)
+			Q.n = 0;
+		__syncthreads();
 	}
 }
 
