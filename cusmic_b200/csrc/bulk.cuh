@@ -53,10 +53,10 @@
 // stopped are skipped there) and the ring runs straight through from one item
 // into the next.
 //
-// The Laplacian (src/filters.cuh:86-105): each consumer thread evaluates two
-// column pairs (x, x + 1) and (x + 256, x + 257) and keeps the quarter values
-// of the rows above and at the current row, and the current row's left and
-// right neighbours, in registers.  Differences the reference computes twice
+// The Laplacian (src/filters.cuh:86-105): each consumer thread evaluates four
+// consecutive columns x .. x + 3 (lane ct of the four warps: x = x0 + 4 ct)
+// and keeps the quarter values of the rows above and at the current row, and
+// the current row's left and right neighbours, in registers.  Differences the reference computes twice
 // are computed once: down(y) = q(y) - q(y+1) and up(y+1) = q(y+1) - q(y) are
 // exact negatives of each other in round-to-nearest, and so are right(x) and
 // left(x+1); negation changes at most the sign of a zero difference.

@@ -31,8 +31,9 @@
 // words of the warp's 128 columns are assembled from the lanes' 4-bit groups
 // by shuffles.  Per-frame facts are set once per item and warp.
 //
-// The block floors of error maps depend on the maps only, so floor_kernel runs
-// before this kernel; the hole fill runs after it.
+// The block floors of error maps depend on the maps only, so they are computed
+// before this kernel (prep_init_kernel, with the call's state and zeroing);
+// the hole fill runs after it.
 //
 // Every wait is bounded as in sig_bulk_kernel.  The frames' layout is checked
 // again on the device: a frame that does not satisfy it stops the kernel as a
