@@ -17,9 +17,11 @@ pixels) are larger than the 126 MB L2, so no flush is needed between steps.
   ``e2e_per_frame`` beside it: the reference-facing ``remove_cosmics``, one
   call per frame, every map uploaded with every frame.
 * ``roofline``: the dominant kernel (prepare, the largest share of kernel
-  time): its algorithmic bytes per launch over its CUDA-event duration,
-  against the measured HBM copy bandwidth; ``roofline_sig_bulk`` the same for
-  the dense detection kernel.
+  time; on this stack prepare and the first pass's dense detection run as one
+  kernel, prep_detect_kernel): its algorithmic bytes per launch over its
+  CUDA-event duration, against the measured HBM copy bandwidth;
+  ``roofline_sig_bulk`` the same for the dense detection kernel where it runs
+  on its own (the ragged batch, noise model).
 * ``plain``/``ragged``: the same implementation called once per frame
   (``remove_cosmics_device``) versus one batched plan, on this stack and on
   the ragged 64-frame batch with per-frame scalars.
